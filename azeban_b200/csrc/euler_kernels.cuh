@@ -1,0 +1,593 @@
+// Fused transform passes of the spectral-viscosity incompressible Euler
+// right-hand side, and the plain real/complex transform passes of FFT<Dim>.
+//
+// One 3-D right-hand side (reference: IncompressibleEuler::dudt,
+// include/azeban/equations/incompressible_euler.hpp:103-120) runs as five
+// passes, each one HBM read and one HBM write of the live array:
+//   1 k_cols<PAD,  inverse>  along x: u_hat [3][N][N][Nh] -> A1 [3][M][N][Nh]
+//                            (copy_to_padded along x fused into the loads)
+//   2 k_cols<PAD,  inverse>  along y: A1 -> A2 [3][M][M][Nh]
+//   3 k_rows_product         along z: c2r, max|u|, B = u (x) u, r2c, keep
+//                            k < Nh: A2 -> B1 [6][M][M][Nh]
+//   4 k_cols<TRUNC, forward> along y, keep the N retained rows: B1 -> B2 [6][M][N][Nh]
+//   5 k_fwd_epilogue         along x, keep retained rows, then computeDudt
+//                            (Leray projection of i k.B, spectral viscosity)
+//                            and the SSP-RK3 stage combination: B2 + u -> out
+// 2-D uses passes 1 (along x), 3 (along y) and 5.
+#pragma once
+
+#include "az_types.h"
+#include "fft_core.cuh"
+
+namespace azb {
+
+enum ColMode : int { COL_PLAIN = 0, COL_PAD = 1, COL_TRUNC = 2 };
+
+// Padded row m -> source row of an axis of unpadded length n, or -1 for a
+// zero (copy_to_padded_functions.hpp:36-51 in the reference; the Nyquist
+// index n/2 stays on the positive side).
+__device__ __forceinline__ int pad_src_row(int m, int n, int L) {
+  if (m < n / 2 + 1) return m;
+  if (m < n / 2 + 1 + L - n) return -1;
+  return m - (L - n);
+}
+
+// Padded row m -> retained row of the unpadded axis, or -1 if dropped
+// (inverse of i_B = i >= n/2+1 ? L - n + i : i, incompressible_euler.hpp:294-299).
+__device__ __forceinline__ int retained_row(int m, int n, int L) {
+  if (m <= n / 2) return m;
+  if (m >= L - n / 2 + 1) return m - (L - n);
+  return -1;
+}
+
+struct ColArgs {
+  const void* in;
+  void* out;
+  const void* tw;
+  long long ninner;  // contiguous columns per slab
+  int ntile;         // ceil(ninner / NC)
+  int n_short;       // unpadded length (input rows for PAD, output rows for TRUNC)
+  long long in_row, out_row;
+  long long in_outer, out_outer;
+  long long in_comp, out_comp;
+  long long in_mem, out_mem;
+  Ctrl* ctrl;     // optional: per-member skip flags
+  int clear_max;  // nonzero: also reset the member's CFL accumulator
+};
+
+// Batched column transforms along a strided axis.  grid = (ntile * nouter,
+// ncomp, nmembers); block = NC * L/E threads.
+template <typename T, int L, int NC, int S, int MODE>
+__global__ void __launch_bounds__(NC * Plan<L>::TPL) k_cols(ColArgs a) {
+  using C = cvec<T>;
+  extern __shared__ __align__(16) unsigned char az_smem[];
+  C* tw = reinterpret_cast<C*>(az_smem);
+  C* sm = tw + L;
+  const int member = blockIdx.z;
+  if (a.ctrl != nullptr) {
+    if (a.ctrl[member].skip) return;
+    // The CFL accumulator is read only after the product pass of this
+    // right-hand side, which runs after this kernel.
+    if (a.clear_max && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
+      a.ctrl[member].umax64 = 0ull;
+      a.ctrl[member].umax32 = 0u;
+    }
+  }
+  const int tile = blockIdx.x % a.ntile;
+  const int outer = blockIdx.x / a.ntile;
+  const int comp = blockIdx.y;
+  const int col = threadIdx.x % NC;
+  const int tl = threadIdx.x / NC;
+  const long long p = (long long)tile * NC + col;
+  const bool valid = p < a.ninner;
+  const C* in = reinterpret_cast<const C*>(a.in) + member * a.in_mem + comp * a.in_comp +
+                outer * a.in_outer + p;
+  C* out = reinterpret_cast<C*>(a.out) + member * a.out_mem + comp * a.out_comp +
+           outer * a.out_outer + p;
+  load_twiddles<C, L>(tw, reinterpret_cast<const C*>(a.tw));
+  __syncthreads();
+  const int n = a.n_short;
+  auto load = [&](int m) -> C {
+    int src = m;
+    if constexpr (MODE == COL_PAD) src = pad_src_row(m, n, L);
+    if (!valid || src < 0) return cmk<C>(T(0), T(0));
+    return in[src * a.in_row];
+  };
+  auto store = [&](int m, C v) {
+    int dst = m;
+    if constexpr (MODE == COL_TRUNC) dst = retained_row(m, n, L);
+    if (valid && dst >= 0) out[dst * a.out_row] = v;
+  };
+  fft_columns<C, S, L, NC, false>(sm, tw, col, tl, load, store);
+}
+
+struct RowArgs {
+  const void* in;
+  void* out;
+  const void* tw;
+  long long nlines;  // lines per member
+  int nh;            // complex entries per spectral line (N/2+1)
+  long long in_line, out_line;
+  long long in_comp, out_comp;
+  long long in_mem, out_mem;
+  double norm;  // 1 / (N^{d/2} M^{d/2})
+  Ctrl* ctrl;
+};
+
+template <typename T> __device__ __forceinline__ void atomic_max_abs(Ctrl* c, T v);
+template <> __device__ __forceinline__ void atomic_max_abs<double>(Ctrl* c, double v) {
+  atomicMax(&c->umax64, (unsigned long long)__double_as_longlong(v));
+}
+template <> __device__ __forceinline__ void atomic_max_abs<float>(Ctrl* c, float v) {
+  atomicMax(&c->umax32, __float_as_uint(v));
+}
+
+// Hermitian extension of a half spectrum: bin m of the length-L spectrum of a
+// real signal whose bins [0, nh) are stored at `line` (nullptr: all zero).
+// The imaginary parts of bin 0 and of bin L/2 are dropped, as a c2r does.
+template <typename C, int L>
+__device__ __forceinline__ C herm_bin(const C* line, int nh, int m) {
+  using T = decltype(C::x);
+  const bool mirror = m > L / 2;
+  const int mm = mirror ? L - m : m;
+  C v = cmk<C>(T(0), T(0));
+  if (line != nullptr && mm < nh) v = line[mm];
+  if (mirror) v.y = -v.y;
+  if (m == 0 || 2 * m == L) v.y = T(0);
+  return v;
+}
+
+// Contiguous-axis pass of the right-hand side: for each pair of lines, the
+// inverse real transform of the DIM velocity components (two real signals per
+// complex transform), the CFL maximum, the products B = u (x) u in the
+// reference's component order, and the forward real transform of the
+// products, of which only bins [0, nh) are written.
+// grid = (ceil(nlines / (2 NLP)), nmembers); block = NB * NLP * L/E.
+template <typename T, int L, int NLP, int DIM>
+__global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NLP * Plan<L>::TPL)
+    k_rows_product(RowArgs a) {
+  using C = cvec<T>;
+  constexpr int NB = DIM * (DIM + 1) / 2;
+  constexpr int NINV = DIM * NLP;
+  constexpr int NFWD = NB * NLP;
+  constexpr int SROW = NFWD + 1;
+  constexpr int TPL = Plan<L>::TPL;
+  constexpr int NT = NFWD * TPL;
+  extern __shared__ __align__(16) unsigned char az_smem[];
+  C* tw = reinterpret_cast<C*>(az_smem);
+  C* sm = tw + L;
+  const int member = blockIdx.y;
+  Ctrl* ctrl = a.ctrl + member;
+  if (ctrl->skip) return;
+  const int tid = threadIdx.x;
+  const long long line0 = (long long)blockIdx.x * 2 * NLP;
+  const C* in = reinterpret_cast<const C*>(a.in) + member * a.in_mem;
+  C* out = reinterpret_cast<C*>(a.out) + member * a.out_mem;
+  load_twiddles<C, L>(tw, reinterpret_cast<const C*>(a.tw));
+
+  // 1. Load and pack: column (p, q) holds signal 2q + i * signal 2q+1 of the
+  //    line pair p, signal s = component s % DIM of line (s / DIM).
+  for (int idx = tid; idx < NINV * L; idx += NT) {
+    const int m = idx % L;
+    const int cz = idx / L;
+    const int p = cz / DIM;
+    const int q = cz % DIM;
+    C x[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int s = 2 * q + h;
+      const long long ln = line0 + 2 * p + s / DIM;
+      const C* src = ln < a.nlines ? in + (s % DIM) * a.in_comp + ln * a.in_line : nullptr;
+      x[h] = herm_bin<C, L>(src, a.nh, m);
+    }
+    sm[m * SROW + cz] = cmk<C>(x[0].x - x[1].y, x[0].y + x[1].x);
+  }
+  __syncthreads();
+
+  // 2. Inverse transforms of the NINV packed columns.
+  {
+    const bool active = tid < NINV * TPL;
+    const int col = active ? tid % NINV : 0;
+    const int tl = active ? tid / NINV : 0;
+    fft_columns<C, +1, L, SROW, true>(
+        sm, tw, col, tl, [&](int m) { return sm[m * SROW + col]; },
+        [&](int m, C v) {
+          if (active) sm[m * SROW + col] = v;
+        });
+  }
+  __syncthreads();
+
+  // 3. CFL maximum and products.
+  constexpr int MAXI = (NLP * L + NT - 1) / NT;
+  T sv[MAXI][2 * DIM];
+  T vmax = T(0);
+  bool bad = false;
+#pragma unroll
+  for (int it = 0; it < MAXI; ++it) {
+    const int idx = tid + it * NT;
+    if (idx < NLP * L) {
+      const int m = idx % L;
+      const int p = idx / L;
+#pragma unroll
+      for (int q = 0; q < DIM; ++q) {
+        const C z = sm[m * SROW + p * DIM + q];
+        sv[it][2 * q] = z.x;
+        sv[it][2 * q + 1] = z.y;
+      }
+#pragma unroll
+      for (int s = 0; s < 2 * DIM; ++s) {
+        const T av = fabs(sv[it][s]);
+        bad |= !isfinite(av);
+        vmax = fmax(vmax, av);
+      }
+    }
+  }
+  __syncthreads();
+  const T norm = T(a.norm);
+#pragma unroll
+  for (int it = 0; it < MAXI; ++it) {
+    const int idx = tid + it * NT;
+    if (idx < NLP * L) {
+      const int m = idx % L;
+      const int p = idx / L;
+      T pa[NB], pb[NB];
+      if constexpr (DIM == 2) {
+        const T a1 = norm * sv[it][0], a2 = norm * sv[it][1];
+        const T b1 = norm * sv[it][2], b2 = norm * sv[it][3];
+        pa[0] = a1 * a1; pa[1] = a1 * a2; pa[2] = a2 * a2;
+        pb[0] = b1 * b1; pb[1] = b1 * b2; pb[2] = b2 * b2;
+      } else {
+        const T a1 = norm * sv[it][0], a2 = norm * sv[it][1], a3 = norm * sv[it][2];
+        const T b1 = norm * sv[it][3], b2 = norm * sv[it][4], b3 = norm * sv[it][5];
+        pa[0] = a1 * a1; pa[1] = a2 * a1; pa[2] = a2 * a2;
+        pa[3] = a3 * a1; pa[4] = a3 * a2; pa[5] = a3 * a3;
+        pb[0] = b1 * b1; pb[1] = b2 * b1; pb[2] = b2 * b2;
+        pb[3] = b3 * b1; pb[4] = b3 * b2; pb[5] = b3 * b3;
+      }
+#pragma unroll
+      for (int c = 0; c < NB; ++c) sm[m * SROW + p * NB + c] = cmk<C>(pa[c], pb[c]);
+    }
+  }
+  __syncthreads();
+
+  // 4. Forward transforms of the NFWD product columns (product c of line a
+  //    in the real part, of line b in the imaginary part).
+  {
+    const int col = tid % NFWD;
+    const int tl = tid / NFWD;
+    fft_columns<C, -1, L, SROW, true>(
+        sm, tw, col, tl, [&](int m) { return sm[m * SROW + col]; },
+        [&](int m, C v) { sm[m * SROW + col] = v; });
+  }
+  __syncthreads();
+
+  // 5. Separate the two real spectra and write bins [0, nh).
+  for (int idx = tid; idx < NFWD * a.nh; idx += NT) {
+    const int k = idx % a.nh;
+    const int cf = idx / a.nh;
+    const int p = cf / NB;
+    const int c = cf % NB;
+    const C fk = sm[k * SROW + cf];
+    const C fm = sm[((L - k) % L) * SROW + cf];
+    const C xa = cmk<C>(T(0.5) * (fk.x + fm.x), T(0.5) * (fk.y - fm.y));
+    const C xb = cmk<C>(T(0.5) * (fk.y + fm.y), T(-0.5) * (fk.x - fm.x));
+    const long long la = line0 + 2 * p;
+    if (la < a.nlines) out[c * a.out_comp + la * a.out_line + k] = xa;
+    if (la + 1 < a.nlines) out[c * a.out_comp + (la + 1) * a.out_line + k] = xb;
+  }
+
+  // CFL reduction: warp, then block, then one atomic per CTA.
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) vmax = fmax(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+  const unsigned anybad = __any_sync(0xffffffffu, bad);
+  __shared__ T red[32];
+  __shared__ int redbad;
+  if (tid == 0) redbad = 0;
+  __syncthreads();
+  if ((tid & 31) == 0) {
+    red[tid >> 5] = vmax;
+    if (anybad) redbad = 1;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    T m = T(0);
+    for (int w = 0; w < (NT + 31) / 32; ++w) m = fmax(m, red[w]);
+    atomic_max_abs<T>(ctrl, m);
+    if (redbad) atomicOr(&ctrl->err, 1);
+  }
+}
+
+struct EpiArgs {
+  const void* B;
+  const void* u;
+  const void* u0;
+  void* out;
+  const void* tw;
+  long long ninner;  // modes per retained row: N*Nh (3-D) or Nh (2-D)
+  int ntile;
+  int N, nh;
+  long long B_row, B_comp, B_mem;
+  long long u_row, u_comp, u_mem;
+  int mode;
+  Visc visc;
+  const Ctrl* ctrl;
+};
+
+// nu(|k|) of the reference's viscosity laws
+// (include/azeban/equations/spectral_viscosity.hpp:27-123).
+template <typename T> __device__ __forceinline__ T visc_eval(const Visc& v, T k) {
+  switch (v.type) {
+    case VISC_SMOOTH_CUTOFF:
+    case VISC_STEP: {
+      T q;
+      if (v.type == VISC_SMOOTH_CUTOFF) {
+        const T k1 = fabs(k) / T(v.k0);
+        const T k2 = k1 * k1;
+        const T k4 = k2 * k2;
+        const T k8 = k4 * k4;
+        const T k16 = k8 * k8;
+        const T k18 = k16 * k2;
+        q = T(1) - exp(-k18);
+      } else {
+        q = fabs(k) > T(v.k0) ? T(1) : T(0);
+      }
+      const T pk = (v.s == 1.0) ? k * k : T(pow(k, T(2 * v.s)));
+      return -T(v.eps) * pk * q;
+    }
+    case VISC_QUADRATIC: {
+      const T knorm = k / T(2 * 3.14159265358979323846);
+      return -T(v.eps) * fmax(T(0), knorm * knorm - T(v.N));
+    }
+    default:
+      return T(0);
+  }
+}
+
+// Forward transform along x of the NB product components, kept at the N
+// retained rows, then per mode: L = (I - k k^T/|k|^2)(i k.B_hat),
+// dudt = |k| = 0 ? 0 : -L + nu(|k|) u_hat (incompressible_euler.hpp:230-347,
+// incompressible_euler_functions.hpp:47-112), then the stage combination:
+//   MODE_DUDT: out = dudt
+//   MODE_RK1:  out = u + dt dudt                      (ssp_rk3.hpp:55)
+//   MODE_RK2:  out = 3/4 u0 + 1/4 (u + dt dudt)       (ssp_rk3.hpp:57-58)
+//   MODE_RK3:  out = 2/3 (u + dt dudt) + 1/3 u0       (ssp_rk3.hpp:60-61)
+// grid = (ntile, nmembers); block = NB * NCM * L/E.
+template <typename T, int L, int NCM, int DIM>
+__global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NCM * Plan<L>::TPL)
+    k_fwd_epilogue(EpiArgs a) {
+  using C = cvec<T>;
+  constexpr int NB = DIM * (DIM + 1) / 2;
+  constexpr int NC = NB * NCM;
+  constexpr int SROW = NC;
+  constexpr int TPL = Plan<L>::TPL;
+  constexpr int NT = NC * TPL;
+  extern __shared__ __align__(16) unsigned char az_smem[];
+  C* tw = reinterpret_cast<C*>(az_smem);
+  C* sm = tw + L;
+  const int member = blockIdx.y;
+  if (a.ctrl != nullptr && a.ctrl[member].skip) return;
+  const int tid = threadIdx.x;
+  const int tile = blockIdx.x;
+  const int N = a.N;
+  load_twiddles<C, L>(tw, reinterpret_cast<const C*>(a.tw));
+  __syncthreads();
+  {
+    const int col = tid % NC;
+    const int tl = tid / NC;
+    const int c = col / NCM;
+    const int pl = col % NCM;
+    const long long p = (long long)tile * NCM + pl;
+    const bool valid = p < a.ninner;
+    const C* Bp = reinterpret_cast<const C*>(a.B) + member * a.B_mem + c * a.B_comp + p;
+    fft_columns<C, -1, L, SROW, true>(
+        sm, tw, col, tl,
+        [&](int m) -> C { return valid ? Bp[m * a.B_row] : cmk<C>(T(0), T(0)); },
+        [&](int m, C v) {
+          const int i = retained_row(m, N, L);
+          if (i >= 0) sm[i * SROW + col] = v;
+        });
+  }
+  __syncthreads();
+
+  const double dtd = (a.mode != MODE_DUDT && a.ctrl != nullptr) ? a.ctrl[member].dt : 0.0;
+  const T dt = T(dtd);
+  const T twopi = T(2 * 3.14159265358979323846);
+  const C* u = reinterpret_cast<const C*>(a.u) + member * a.u_mem;
+  const C* u0 = reinterpret_cast<const C*>(a.u0) + member * a.u_mem;
+  C* out = reinterpret_cast<C*>(a.out) + member * a.u_mem;
+  for (int idx = tid; idx < N * NCM; idx += NT) {
+    const int pl = idx % NCM;
+    const int i = idx / NCM;
+    const long long p = (long long)tile * NCM + pl;
+    if (p >= a.ninner) continue;
+    const int i_ = i >= N / 2 + 1 ? i - N : i;
+    C Bv[NB];
+#pragma unroll
+    for (int c = 0; c < NB; ++c) Bv[c] = sm[i * SROW + c * NCM + pl];
+    const long long off = (long long)i * a.u_row + p;
+    C uv[DIM];
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) uv[c] = u[c * a.u_comp + off];
+    C Lh[DIM];
+    T absk2;
+    if constexpr (DIM == 2) {
+      const int kk = (int)p;
+      const T k1 = twopi * T(i_);
+      const T k2 = twopi * T(kk);
+      absk2 = k1 * k1 + k2 * k2;
+      // b = i k.B (force = 0)
+      const C b1 = cmk<C>(-k1 * Bv[0].y - k2 * Bv[1].y, k1 * Bv[0].x + k2 * Bv[1].x);
+      const C b2 = cmk<C>(-k1 * Bv[1].y - k2 * Bv[2].y, k1 * Bv[1].x + k2 * Bv[2].x);
+      const T inv = T(1) / absk2;
+      const T k11 = k1 * k1 * inv, k12 = k1 * k2 * inv, k22 = k2 * k2 * inv;
+      const T c11 = T(1) - k11, c12 = T(0) - k12, c22 = T(1) - k22;
+      Lh[0] = cmk<C>(c11 * b1.x + c12 * b2.x, c11 * b1.y + c12 * b2.y);
+      Lh[1] = cmk<C>(c12 * b1.x + c22 * b2.x, c12 * b1.y + c22 * b2.y);
+    } else {
+      const int j = (int)(p / a.nh);
+      const int kk = (int)(p % a.nh);
+      const int j_ = j >= N / 2 + 1 ? j - N : j;
+      const T k1 = twopi * T(i_);
+      const T k2 = twopi * T(j_);
+      const T k3 = twopi * T(kk);
+      absk2 = k1 * k1 + k2 * k2 + k3 * k3;
+      // B order: 0 B11, 1 B21, 2 B22, 3 B31, 4 B32, 5 B33
+      const C b1 = cmk<C>(-k1 * Bv[0].y - k2 * Bv[1].y - k3 * Bv[3].y,
+                          k1 * Bv[0].x + k2 * Bv[1].x + k3 * Bv[3].x);
+      const C b2 = cmk<C>(-k1 * Bv[1].y - k2 * Bv[2].y - k3 * Bv[4].y,
+                          k1 * Bv[1].x + k2 * Bv[2].x + k3 * Bv[4].x);
+      const C b3 = cmk<C>(-k1 * Bv[3].y - k2 * Bv[4].y - k3 * Bv[5].y,
+                          k1 * Bv[3].x + k2 * Bv[4].x + k3 * Bv[5].x);
+      const T inv = T(1) / absk2;
+      const T k11 = k1 * k1 * inv, k12 = k1 * k2 * inv, k13 = k1 * k3 * inv;
+      const T k22 = k2 * k2 * inv, k23 = k2 * k3 * inv, k33 = k3 * k3 * inv;
+      const T c11 = T(1) - k11, c12 = T(0) - k12, c13 = T(0) - k13;
+      const T c22 = T(1) - k22, c23 = T(0) - k23, c33 = T(1) - k33;
+      Lh[0] = cmk<C>(c11 * b1.x + c12 * b2.x + c13 * b3.x, c11 * b1.y + c12 * b2.y + c13 * b3.y);
+      Lh[1] = cmk<C>(c12 * b1.x + c22 * b2.x + c23 * b3.x, c12 * b1.y + c22 * b2.y + c23 * b3.y);
+      Lh[2] = cmk<C>(c13 * b1.x + c23 * b2.x + c33 * b3.x, c13 * b1.y + c23 * b2.y + c33 * b3.y);
+    }
+    const T nu = visc_eval<T>(a.visc, sqrt(absk2));
+    const bool zero = absk2 == T(0);
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+      const C d = zero ? cmk<C>(T(0), T(0))
+                       : cmk<C>(-Lh[c].x + nu * uv[c].x, -Lh[c].y + nu * uv[c].y);
+      C r;
+      if (a.mode == MODE_DUDT) {
+        r = d;
+      } else {
+        const C t = cmk<C>(uv[c].x + dt * d.x, uv[c].y + dt * d.y);
+        if (a.mode == MODE_RK1) {
+          r = t;
+        } else {
+          const C w = u0[c * a.u_comp + off];
+          if (a.mode == MODE_RK2) {
+            r = cmk<C>(T(0.75) * w.x + T(0.25) * t.x, T(0.75) * w.y + T(0.25) * t.y);
+          } else {
+            const T c23 = T(2.0 / 3.0), c13 = T(1.0 / 3.0);
+            r = cmk<C>(c23 * t.x + c13 * w.x, c23 * t.y + c13 * w.y);
+          }
+        }
+      }
+      out[c * a.u_comp + off] = r;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Plain real <-> complex transforms along the contiguous axis (FFT<Dim>).
+// Two real lines share one complex transform.
+// ---------------------------------------------------------------------------
+struct RealRowArgs {
+  const void* in;
+  void* out;
+  const void* tw;
+  long long nlines;
+  long long in_line, out_line;  // in elements of the respective type
+};
+
+// c2r: lines of L/2+1 complex -> L real.  grid = ceil(nlines / (2 NLP)).
+template <typename T, int L, int NLP>
+__global__ void __launch_bounds__(NLP * Plan<L>::TPL) k_rows_c2r(RealRowArgs a) {
+  using C = cvec<T>;
+  constexpr int SROW = NLP + 1;
+  constexpr int NT = NLP * Plan<L>::TPL;
+  constexpr int LH = L / 2 + 1;
+  extern __shared__ __align__(16) unsigned char az_smem[];
+  C* tw = reinterpret_cast<C*>(az_smem);
+  C* sm = tw + L;
+  const int tid = threadIdx.x;
+  const long long line0 = (long long)blockIdx.x * 2 * NLP;
+  const C* in = reinterpret_cast<const C*>(a.in);
+  T* out = reinterpret_cast<T*>(a.out);
+  load_twiddles<C, L>(tw, reinterpret_cast<const C*>(a.tw));
+  for (int idx = tid; idx < NLP * L; idx += NT) {
+    const int m = idx % L;
+    const int p = idx / L;
+    const long long la = line0 + 2 * p;
+    const C xa = herm_bin<C, L>(la < a.nlines ? in + la * a.in_line : nullptr, LH, m);
+    const C xb = herm_bin<C, L>(la + 1 < a.nlines ? in + (la + 1) * a.in_line : nullptr, LH, m);
+    sm[m * SROW + p] = cmk<C>(xa.x - xb.y, xa.y + xb.x);
+  }
+  __syncthreads();
+  {
+    const int col = tid % NLP;
+    const int tl = tid / NLP;
+    fft_columns<C, +1, L, SROW, true>(
+        sm, tw, col, tl, [&](int m) { return sm[m * SROW + col]; },
+        [&](int m, C v) { sm[m * SROW + col] = v; });
+  }
+  __syncthreads();
+  for (int idx = tid; idx < 2 * NLP * L; idx += NT) {
+    const int m = idx % L;
+    const int ln = idx / L;
+    const long long line = line0 + ln;
+    if (line < a.nlines) {
+      const C z = sm[m * SROW + ln / 2];
+      out[line * a.out_line + m] = (ln & 1) ? z.y : z.x;
+    }
+  }
+}
+
+// r2c: lines of L real -> L/2+1 complex.  grid = ceil(nlines / (2 NLP)).
+template <typename T, int L, int NLP>
+__global__ void __launch_bounds__(NLP * Plan<L>::TPL) k_rows_r2c(RealRowArgs a) {
+  using C = cvec<T>;
+  constexpr int SROW = NLP + 1;
+  constexpr int NT = NLP * Plan<L>::TPL;
+  constexpr int LH = L / 2 + 1;
+  extern __shared__ __align__(16) unsigned char az_smem[];
+  C* tw = reinterpret_cast<C*>(az_smem);
+  C* sm = tw + L;
+  T* smr = reinterpret_cast<T*>(sm);
+  const int tid = threadIdx.x;
+  const long long line0 = (long long)blockIdx.x * 2 * NLP;
+  const T* in = reinterpret_cast<const T*>(a.in);
+  C* out = reinterpret_cast<C*>(a.out);
+  load_twiddles<C, L>(tw, reinterpret_cast<const C*>(a.tw));
+  for (int idx = tid; idx < 2 * NLP * L; idx += NT) {
+    const int m = idx % L;
+    const int ln = idx / L;
+    const long long line = line0 + ln;
+    const T x = line < a.nlines ? in[line * a.in_line + m] : T(0);
+    smr[2 * (m * SROW + ln / 2) + (ln & 1)] = x;
+  }
+  __syncthreads();
+  {
+    const int col = tid % NLP;
+    const int tl = tid / NLP;
+    fft_columns<C, -1, L, SROW, true>(
+        sm, tw, col, tl, [&](int m) { return sm[m * SROW + col]; },
+        [&](int m, C v) { sm[m * SROW + col] = v; });
+  }
+  __syncthreads();
+  for (int idx = tid; idx < NLP * LH; idx += NT) {
+    const int k = idx % LH;
+    const int p = idx / LH;
+    const C fk = sm[k * SROW + p];
+    const C fm = sm[((L - k) % L) * SROW + p];
+    const long long la = line0 + 2 * p;
+    if (la < a.nlines)
+      out[la * a.out_line + k] = cmk<C>(T(0.5) * (fk.x + fm.x), T(0.5) * (fk.y - fm.y));
+    if (la + 1 < a.nlines)
+      out[(la + 1) * a.out_line + k] = cmk<C>(T(0.5) * (fk.y + fm.y), T(-0.5) * (fk.x - fm.x));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Control kernels: one thread per solve.
+// ---------------------------------------------------------------------------
+// Start of a step with a host-given max_dt (TimeIntegrator::integrate).
+__global__ void k_ctrl_begin_host(Ctrl* c, int n, double max_dt);
+// Start of a step inside simulate_until: max_dt = min(t_end - time, cap)
+// (src/azeban/simulation.cpp:91-95); a finished solve is marked skip.
+__global__ void k_ctrl_begin_sim(Ctrl* c, int n, double cap);
+// Clears the CFL accumulator before a right-hand side.
+__global__ void k_ctrl_clear_max(Ctrl* c, int n);
+// dt = min(C / (N u_max), max_dt), u_max = max / M^d (incompressible_euler.hpp:116-124).
+__global__ void k_ctrl_dt(Ctrl* c, int n, double C, double Nphys, double Md, int fp32);
+// time += dt for every solve that stepped (simulation.cpp:100).
+__global__ void k_ctrl_end(Ctrl* c, int n);
+
+}  // namespace azb

@@ -1,0 +1,3 @@
+// Kernel set for f32 transforms of length 4.
+#include "kernel_set.cuh"
+AZB_INSTANTIATE(float, f32, 4)

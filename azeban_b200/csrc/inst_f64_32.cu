@@ -1,0 +1,3 @@
+// Kernel set for f64 transforms of length 32.
+#include "kernel_set.cuh"
+AZB_INSTANTIATE(double, f64, 32)

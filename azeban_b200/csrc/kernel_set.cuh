@@ -1,0 +1,163 @@
+// Launchers for every pass kernel of one (precision, transform length L).
+// Each instantiation unit (inst_<prec>_<L>.cu) compiles one KernelSet, so the
+// build parallelises over lengths.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "euler_kernels.cuh"
+
+namespace azb {
+
+enum ColKind : int { COLK_PAD_INV = 0, COLK_PLAIN_INV = 1, COLK_TRUNC_FWD = 2, COLK_PLAIN_FWD = 3 };
+
+// Tile shapes of one (precision, L).  Threads per CTA and shared memory
+// follow from them; they are the knobs a tuner turns.
+struct TileShape {
+  int nc;     // columns per CTA, column passes
+  int nlp2;   // line pairs per CTA, 2-D product pass
+  int nlp3;   // line pairs per CTA, 3-D product pass
+  int ncm2;   // modes per CTA, 2-D epilogue pass
+  int ncm3;   // modes per CTA, 3-D epilogue pass
+  int nlpr;   // line pairs per CTA, plain r2c / c2r
+};
+
+struct KernelSet {
+  int L;
+  int precision;  // 0 FP64, 1 FP32
+  TileShape tiles;
+  cudaError_t (*cols)(int kind, const ColArgs&, unsigned gx, unsigned gy, unsigned gz, cudaStream_t);
+  cudaError_t (*rows_product)(int dim, const RowArgs&, unsigned gx, unsigned gy, cudaStream_t);
+  cudaError_t (*epilogue)(int dim, const EpiArgs&, unsigned gx, unsigned gy, cudaStream_t);
+  cudaError_t (*c2r)(const RealRowArgs&, unsigned gx, cudaStream_t);
+  cudaError_t (*r2c)(const RealRowArgs&, unsigned gx, cudaStream_t);
+};
+
+constexpr int kpow2floor(int x) {
+  int p = 1;
+  while (p * 2 <= x) p *= 2;
+  return p;
+}
+constexpr int kclamp(int x, int lo, int hi) { return x < lo ? lo : (x > hi ? hi : x); }
+
+template <typename T, int L> struct Tiles {
+  static constexpr int CB = int(sizeof(cvec<T>));
+  static constexpr int NC = kclamp(kpow2floor(49152 / (L * CB)), 2, 32);
+  static constexpr int NLP3 = kclamp(kpow2floor(81920 / (L * 6 * CB)), 1, 16);
+  static constexpr int NLP2 = kclamp(kpow2floor(81920 / (L * 3 * CB)), 1, 16);
+  static constexpr int NCM3 = kclamp(kpow2floor(81920 / (L * 6 * CB)), 1, 16);
+  static constexpr int NCM2 = kclamp(kpow2floor(81920 / (L * 3 * CB)), 1, 16);
+  static constexpr int NLPR = kclamp(kpow2floor(49152 / (L * CB)), 1, 64);
+};
+
+template <typename K> inline cudaError_t set_smem(K kernel, size_t bytes) {
+  if (bytes <= 48 * 1024) return cudaSuccess;
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+}
+
+template <typename T, int L> struct Launch {
+  using C = cvec<T>;
+  using TS = Tiles<T, L>;
+  static constexpr int TPL = Plan<L>::TPL;
+
+  template <int S, int MODE>
+  static cudaError_t col_kernel(const ColArgs& a, dim3 g, cudaStream_t st) {
+    constexpr int NC = TS::NC;
+    const size_t smem = size_t(L + L * NC) * sizeof(C);
+    auto k = k_cols<T, L, NC, S, MODE>;
+    static const cudaError_t attr = set_smem(k, smem);
+    if (attr != cudaSuccess) return attr;
+    k<<<g, NC * TPL, smem, st>>>(a);
+    return cudaGetLastError();
+  }
+
+  static cudaError_t cols(int kind, const ColArgs& a, unsigned gx, unsigned gy, unsigned gz,
+                          cudaStream_t st) {
+    const dim3 g(gx, gy, gz);
+    switch (kind) {
+      case COLK_PAD_INV: return col_kernel<+1, COL_PAD>(a, g, st);
+      case COLK_PLAIN_INV: return col_kernel<+1, COL_PLAIN>(a, g, st);
+      case COLK_TRUNC_FWD: return col_kernel<-1, COL_TRUNC>(a, g, st);
+      case COLK_PLAIN_FWD: return col_kernel<-1, COL_PLAIN>(a, g, st);
+      default: return cudaErrorInvalidValue;
+    }
+  }
+
+  template <int DIM, int NLP>
+  static cudaError_t rows_kernel(const RowArgs& a, dim3 g, cudaStream_t st) {
+    constexpr int NB = DIM * (DIM + 1) / 2;
+    const size_t smem = size_t(L + L * (NB * NLP + 1)) * sizeof(C);
+    auto k = k_rows_product<T, L, NLP, DIM>;
+    static const cudaError_t attr = set_smem(k, smem);
+    if (attr != cudaSuccess) return attr;
+    k<<<g, NB * NLP * TPL, smem, st>>>(a);
+    return cudaGetLastError();
+  }
+
+  static cudaError_t rows_product(int dim, const RowArgs& a, unsigned gx, unsigned gy,
+                                  cudaStream_t st) {
+    const dim3 g(gx, gy, 1);
+    if (dim == 2) return rows_kernel<2, TS::NLP2>(a, g, st);
+    if (dim == 3) return rows_kernel<3, TS::NLP3>(a, g, st);
+    return cudaErrorInvalidValue;
+  }
+
+  template <int DIM, int NCM>
+  static cudaError_t epi_kernel(const EpiArgs& a, dim3 g, cudaStream_t st) {
+    constexpr int NB = DIM * (DIM + 1) / 2;
+    const size_t smem = size_t(L + L * NB * NCM) * sizeof(C);
+    auto k = k_fwd_epilogue<T, L, NCM, DIM>;
+    static const cudaError_t attr = set_smem(k, smem);
+    if (attr != cudaSuccess) return attr;
+    k<<<g, NB * NCM * TPL, smem, st>>>(a);
+    return cudaGetLastError();
+  }
+
+  static cudaError_t epilogue(int dim, const EpiArgs& a, unsigned gx, unsigned gy,
+                              cudaStream_t st) {
+    const dim3 g(gx, gy, 1);
+    if (dim == 2) return epi_kernel<2, TS::NCM2>(a, g, st);
+    if (dim == 3) return epi_kernel<3, TS::NCM3>(a, g, st);
+    return cudaErrorInvalidValue;
+  }
+
+  static cudaError_t c2r(const RealRowArgs& a, unsigned gx, cudaStream_t st) {
+    constexpr int NLP = TS::NLPR;
+    const size_t smem = size_t(L + L * (NLP + 1)) * sizeof(C);
+    auto k = k_rows_c2r<T, L, NLP>;
+    static const cudaError_t attr = set_smem(k, smem);
+    if (attr != cudaSuccess) return attr;
+    k<<<gx, NLP * TPL, smem, st>>>(a);
+    return cudaGetLastError();
+  }
+
+  static cudaError_t r2c(const RealRowArgs& a, unsigned gx, cudaStream_t st) {
+    constexpr int NLP = TS::NLPR;
+    const size_t smem = size_t(L + L * (NLP + 1)) * sizeof(C);
+    auto k = k_rows_r2c<T, L, NLP>;
+    static const cudaError_t attr = set_smem(k, smem);
+    if (attr != cudaSuccess) return attr;
+    k<<<gx, NLP * TPL, smem, st>>>(a);
+    return cudaGetLastError();
+  }
+
+  static const KernelSet* get() {
+    static const KernelSet ks = {
+        L,
+        sizeof(T) == 8 ? 0 : 1,
+        {TS::NC, TS::NLP2, TS::NLP3, TS::NCM2, TS::NCM3, TS::NLPR},
+        &cols,
+        &rows_product,
+        &epilogue,
+        &c2r,
+        &r2c};
+    return &ks;
+  }
+};
+
+}  // namespace azb
+
+#define AZB_INSTANTIATE(TYPE, TAG, LEN)                              \
+  namespace azb {                                                    \
+  const KernelSet* kernel_set_##TAG##_##LEN() { return Launch<TYPE, LEN>::get(); } \
+  }

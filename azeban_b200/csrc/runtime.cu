@@ -1,0 +1,975 @@
+// Host runtime behind the C ABI: solve descriptors, workspaces, twiddle
+// tables, and the launch sequences of one right-hand side, one SSP-RK3 step
+// and one simulate_until.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/azeban_b200.h"
+#include "az_types.h"
+#include "kernel_set.cuh"
+
+namespace azb {
+
+#define AZB_LENGTHS(X) \
+  X(4) X(6) X(8) X(12) X(16) X(24) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384) X(512) X(768) X(1024) X(1536)
+
+#define AZB_DECL(LEN)                            \
+  const KernelSet* kernel_set_f64_##LEN();       \
+  const KernelSet* kernel_set_f32_##LEN();
+AZB_LENGTHS(AZB_DECL)
+#undef AZB_DECL
+
+static const KernelSet* kernel_set(int precision, int L) {
+#define AZB_CASE(LEN) \
+  case LEN: return precision == 0 ? kernel_set_f64_##LEN() : kernel_set_f32_##LEN();
+  switch (L) {
+    AZB_LENGTHS(AZB_CASE)
+    default: return nullptr;
+  }
+#undef AZB_CASE
+}
+
+static const int kLengths[] = {
+#define AZB_LIST(LEN) LEN,
+    AZB_LENGTHS(AZB_LIST)
+#undef AZB_LIST
+};
+
+// ---------------------------------------------------------------------------
+// Errors
+// ---------------------------------------------------------------------------
+static thread_local std::string g_err;
+
+static az_status fail(az_status st, const std::string& msg) {
+  g_err = msg;
+  return st;
+}
+
+static az_status cuda_fail(cudaError_t e, const char* what) {
+  return fail(AZ_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define AZB_CUDA(call)                                   \
+  do {                                                   \
+    cudaError_t e_ = (call);                             \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call);  \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// Twiddle tables W_L^m = exp(-2 pi i m / L), one per (device, precision, L),
+// evaluated in long double and rounded once.
+// ---------------------------------------------------------------------------
+static std::mutex g_tw_mutex;
+static std::map<std::tuple<int, int, int>, void*> g_tw;
+
+static az_status twiddles(int precision, int L, const void** out) {
+  int dev = 0;
+  AZB_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(g_tw_mutex);
+  auto key = std::make_tuple(dev, precision, L);
+  auto it = g_tw.find(key);
+  if (it != g_tw.end()) {
+    *out = it->second;
+    return AZ_OK;
+  }
+  const long double pi = 3.141592653589793238462643383279502884L;
+  std::vector<double> h64(2 * L);
+  std::vector<float> h32(2 * L);
+  for (int m = 0; m < L; ++m) {
+    const long double a = -2.0L * pi * (long double)m / (long double)L;
+    long double c = cosl(a), s = sinl(a);
+    // Exact values at the quarter points.
+    if ((4 * m) % L == 0) {
+      const int q = (4 * m) / L;
+      c = (q == 0) ? 1.0L : (q == 2 ? -1.0L : 0.0L);
+      s = (q == 1) ? -1.0L : (q == 3 ? 1.0L : 0.0L);
+    }
+    h64[2 * m] = (double)c;
+    h64[2 * m + 1] = (double)s;
+    h32[2 * m] = (float)c;
+    h32[2 * m + 1] = (float)s;
+  }
+  void* d = nullptr;
+  const size_t bytes = precision == 0 ? h64.size() * sizeof(double) : h32.size() * sizeof(float);
+  AZB_CUDA(cudaMalloc(&d, bytes));
+  AZB_CUDA(cudaMemcpy(d, precision == 0 ? (const void*)h64.data() : (const void*)h32.data(), bytes,
+                      cudaMemcpyHostToDevice));
+  g_tw[key] = d;
+  *out = d;
+  return AZ_OK;
+}
+
+static long long cdiv(long long a, long long b) { return (a + b - 1) / b; }
+
+// ---------------------------------------------------------------------------
+// Optional per-pass timing: each pass launch bracketed by two events on its
+// own stream; durations and algorithmic bytes accumulate per pass id.
+// ---------------------------------------------------------------------------
+enum PassId : int { P_INV_X = 0, P_INV_Y = 1, P_PRODUCT = 2, P_FWD_Y = 3, P_EPILOGUE = 4, P_NPASS = 5 };
+struct ProfRec {
+  int pass;
+  double bytes;
+  cudaEvent_t a, b;
+};
+static bool g_prof = false;
+static std::vector<ProfRec> g_prof_recs;
+static std::vector<cudaEvent_t> g_prof_pool;
+
+static cudaEvent_t prof_event() {
+  if (!g_prof_pool.empty()) {
+    cudaEvent_t e = g_prof_pool.back();
+    g_prof_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  return e;
+}
+
+struct ProfScope {
+  int pass;
+  double bytes;
+  cudaStream_t st;
+  cudaEvent_t a = nullptr;
+  ProfScope(int p, double by, cudaStream_t s) : pass(p), bytes(by), st(s) {
+    if (g_prof) {
+      a = prof_event();
+      cudaEventRecord(a, st);
+    }
+  }
+  ~ProfScope() {
+    if (g_prof && a) {
+      cudaEvent_t b = prof_event();
+      cudaEventRecord(b, st);
+      g_prof_recs.push_back({pass, bytes, a, b});
+    }
+  }
+};
+
+}  // namespace azb
+
+using namespace azb;
+
+// ---------------------------------------------------------------------------
+// Equation
+// ---------------------------------------------------------------------------
+struct az_euler_s {
+  int dim, prec, batch;
+  long long N, M, Nh;
+  Visc visc;
+  double eps_visc;  // Equation::visc()
+  const KernelSet* ks;
+  const void* tw;
+  size_t csize;  // bytes per complex element
+  // workspace: buf0 [6][M][N][Nh] (3-D) | [2][M][Nh] (2-D), buf1, buf2
+  void* work = nullptr;
+  size_t work_bytes = 0;
+  char* buf[3] = {nullptr, nullptr, nullptr};
+  long long buf_mem[3] = {0, 0, 0};  // member strides (elements)
+  long long state_mem;               // member stride of a state array
+  long long state_elems;             // batch * state_mem
+  Ctrl* ctrl = nullptr;              // [batch]
+  double norm;
+  double Md;
+};
+
+const char* az_last_error_string(void) { return g_err.c_str(); }
+
+az_status az_supported_lengths(int* out, int cap, int* n) {
+  const int cnt = int(sizeof(kLengths) / sizeof(kLengths[0]));
+  if (n) *n = cnt;
+  if (out)
+    for (int i = 0; i < cnt && i < cap; ++i) out[i] = kLengths[i];
+  return AZ_OK;
+}
+
+az_status az_euler_create(const az_euler_desc* d, az_euler* out) {
+  if (!d || !out) return fail(AZ_ERR_INVALID, "az_euler_create: null argument");
+  *out = nullptr;
+  if (d->dim != 2 && d->dim != 3) return fail(AZ_ERR_INVALID, "Incompressible Euler is only implemented for 2D and 3D");
+  if (d->N_phys < 2 || (d->N_phys % 2) != 0) return fail(AZ_ERR_INVALID, "N_phys must be even and >= 2");
+  if (d->N_phys_pad < d->N_phys) return fail(AZ_ERR_INVALID, "N_phys_pad must be >= N_phys");
+  if (d->precision != AZ_PREC_F64 && d->precision != AZ_PREC_F32) return fail(AZ_ERR_INVALID, "unknown precision");
+  if (d->batch < 1) return fail(AZ_ERR_INVALID, "batch must be >= 1");
+  if (d->visc.type < 0 || d->visc.type > 3) return fail(AZ_ERR_INVALID, "unknown viscosity type");
+  const KernelSet* ks = kernel_set(d->precision, int(d->N_phys_pad));
+  if (!ks)
+    return fail(AZ_ERR_UNSUPPORTED, "N_phys_pad = " + std::to_string(d->N_phys_pad) +
+                                        " has no compiled transform length");
+  auto* e = new az_euler_s();
+  e->dim = d->dim;
+  e->prec = d->precision;
+  e->batch = d->batch;
+  e->N = d->N_phys;
+  e->M = d->N_phys_pad;
+  e->Nh = e->N / 2 + 1;
+  e->visc.type = d->visc.type;
+  e->visc.eps = d->visc.eps;
+  e->visc.s = d->visc.s;
+  e->visc.k0 = d->visc.k0;
+  e->visc.N = d->visc.N;
+  e->eps_visc = d->visc.type == AZ_VISC_NONE ? 0.0 : d->visc.eps;
+  e->ks = ks;
+  e->csize = d->precision == 0 ? 16 : 8;
+  const long long N = e->N, M = e->M, Nh = e->Nh;
+  if (e->dim == 3) {
+    e->buf_mem[0] = 6 * M * N * Nh;  // A1 [3][M][N][Nh] then B2 [6][M][N][Nh]
+    e->buf_mem[1] = 3 * M * M * Nh;  // A2
+    e->buf_mem[2] = 6 * M * M * Nh;  // B1
+    e->state_mem = 3 * N * N * Nh;
+    e->norm = 1.0 / (std::pow(std::sqrt((double)N), 3) * std::pow(std::sqrt((double)M), 3));
+    e->Md = (double)(M * M * M);
+  } else {
+    e->buf_mem[0] = 2 * M * Nh;  // A1
+    e->buf_mem[1] = 3 * M * Nh;  // B1
+    e->buf_mem[2] = 0;
+    e->state_mem = 2 * N * Nh;
+    e->norm = 1.0 / (std::pow(std::sqrt((double)N), 2) * std::pow(std::sqrt((double)M), 2));
+    e->Md = (double)(M * M);
+  }
+  e->state_elems = e->state_mem * e->batch;
+  size_t off[3];
+  size_t total = 0;
+  for (int b = 0; b < 3; ++b) {
+    off[b] = total;
+    const size_t bytes = size_t(e->buf_mem[b]) * e->batch * e->csize;
+    total += (bytes + 255) / 256 * 256;
+  }
+  az_status st = twiddles(e->prec, int(M), &e->tw);
+  if (st != AZ_OK) {
+    delete e;
+    return st;
+  }
+  cudaError_t ce = cudaMalloc(&e->work, total);
+  if (ce != cudaSuccess) {
+    delete e;
+    cudaGetLastError();
+    return fail(AZ_ERR_NOMEM, "az_euler_create: workspace of " + std::to_string(total) +
+                                  " bytes: " + cudaGetErrorString(ce));
+  }
+  e->work_bytes = total;
+  for (int b = 0; b < 3; ++b) e->buf[b] = static_cast<char*>(e->work) + off[b];
+  ce = cudaMalloc(&e->ctrl, sizeof(Ctrl) * e->batch);
+  if (ce != cudaSuccess) {
+    cudaFree(e->work);
+    delete e;
+    cudaGetLastError();
+    return fail(AZ_ERR_NOMEM, "az_euler_create: control block");
+  }
+  ce = cudaMemset(e->ctrl, 0, sizeof(Ctrl) * e->batch);
+  if (ce != cudaSuccess) {
+    cudaFree(e->work);
+    cudaFree(e->ctrl);
+    delete e;
+    return cuda_fail(ce, "cudaMemset");
+  }
+  *out = e;
+  return AZ_OK;
+}
+
+az_status az_euler_destroy(az_euler e) {
+  if (!e) return AZ_OK;
+  cudaFree(e->work);
+  cudaFree(e->ctrl);
+  delete e;
+  return AZ_OK;
+}
+
+int az_euler_n_vars(az_euler e) { return e ? e->dim : 0; }
+double az_euler_visc(az_euler e) { return e ? e->eps_visc : 0.0; }
+size_t az_euler_workspace_size(az_euler e) { return e ? e->work_bytes : 0; }
+
+namespace azb {
+
+// One right-hand side of every member: out <- stage(mode, u, u0, RHS(u)).
+// first_stage: compute dt = min(C/(N u_max), max_dt) after the product pass.
+static az_status rhs(az_euler e, const void* u, const void* u0, void* out, int mode, bool first_stage,
+                     double C, cudaStream_t st) {
+  const KernelSet* ks = e->ks;
+  const long long N = e->N, M = e->M, Nh = e->Nh;
+  const unsigned B = unsigned(e->batch);
+  const int nc = ks->tiles.nc;
+  cudaError_t ce;
+  if (e->dim == 3) {
+    // pass 1: inverse along x with padding, state -> A1 [3][M][N][Nh]
+    ColArgs a1{};
+    a1.in = u;
+    a1.out = e->buf[0];
+    a1.tw = e->tw;
+    a1.ninner = N * Nh;
+    a1.ntile = int(cdiv(a1.ninner, nc));
+    a1.n_short = int(N);
+    a1.in_row = N * Nh;
+    a1.out_row = N * Nh;
+    a1.in_comp = N * N * Nh;
+    a1.out_comp = M * N * Nh;
+    a1.in_mem = e->state_mem;
+    a1.out_mem = e->buf_mem[0];
+    a1.ctrl = e->ctrl;
+    a1.clear_max = 1;
+    {
+      ProfScope ps(P_INV_X, double(B) * 3 * (N * N * Nh + M * N * Nh) * e->csize, st);
+      ce = ks->cols(COLK_PAD_INV, a1, unsigned(a1.ntile), 3, B, st);
+    }
+    if (ce != cudaSuccess) return cuda_fail(ce, "rhs pass 1");
+    // pass 2: inverse along y with padding, A1 -> A2 [3][M][M][Nh]
+    ColArgs a2{};
+    a2.in = e->buf[0];
+    a2.out = e->buf[1];
+    a2.tw = e->tw;
+    a2.ninner = Nh;
+    a2.ntile = int(cdiv(Nh, nc));
+    a2.n_short = int(N);
+    a2.in_row = Nh;
+    a2.out_row = Nh;
+    a2.in_outer = N * Nh;
+    a2.out_outer = M * Nh;
+    a2.in_comp = M * N * Nh;
+    a2.out_comp = M * M * Nh;
+    a2.in_mem = e->buf_mem[0];
+    a2.out_mem = e->buf_mem[1];
+    a2.ctrl = e->ctrl;
+    {
+      ProfScope ps(P_INV_Y, double(B) * 3 * (M * N * Nh + M * M * Nh) * e->csize, st);
+      ce = ks->cols(COLK_PAD_INV, a2, unsigned(a2.ntile * M), 3, B, st);
+    }
+    if (ce != cudaSuccess) return cuda_fail(ce, "rhs pass 2");
+    // pass 3: z lines, product, CFL max: A2 -> B1 [6][M][M][Nh]
+    RowArgs r{};
+    r.in = e->buf[1];
+    r.out = e->buf[2];
+    r.tw = e->tw;
+    r.nlines = M * M;
+    r.nh = int(Nh);
+    r.in_line = Nh;
+    r.out_line = Nh;
+    r.in_comp = M * M * Nh;
+    r.out_comp = M * M * Nh;
+    r.in_mem = e->buf_mem[1];
+    r.out_mem = e->buf_mem[2];
+    r.norm = e->norm;
+    r.ctrl = e->ctrl;
+    {
+      ProfScope ps(P_PRODUCT, double(B) * 9 * (M * M * Nh) * e->csize, st);
+      ce = ks->rows_product(3, r, unsigned(cdiv(r.nlines, 2 * ks->tiles.nlp3)), B, st);
+    }
+    if (ce != cudaSuccess) return cuda_fail(ce, "rhs pass 3");
+  } else {
+    ColArgs a1{};
+    a1.in = u;
+    a1.out = e->buf[0];
+    a1.tw = e->tw;
+    a1.ninner = Nh;
+    a1.ntile = int(cdiv(Nh, nc));
+    a1.n_short = int(N);
+    a1.in_row = Nh;
+    a1.out_row = Nh;
+    a1.in_comp = N * Nh;
+    a1.out_comp = M * Nh;
+    a1.in_mem = e->state_mem;
+    a1.out_mem = e->buf_mem[0];
+    a1.ctrl = e->ctrl;
+    a1.clear_max = 1;
+    {
+      ProfScope ps(P_INV_X, double(B) * 2 * (N * Nh + M * Nh) * e->csize, st);
+      ce = ks->cols(COLK_PAD_INV, a1, unsigned(a1.ntile), 2, B, st);
+    }
+    if (ce != cudaSuccess) return cuda_fail(ce, "rhs pass 1 (2-D)");
+    RowArgs r{};
+    r.in = e->buf[0];
+    r.out = e->buf[1];
+    r.tw = e->tw;
+    r.nlines = M;
+    r.nh = int(Nh);
+    r.in_line = Nh;
+    r.out_line = Nh;
+    r.in_comp = M * Nh;
+    r.out_comp = M * Nh;
+    r.in_mem = e->buf_mem[0];
+    r.out_mem = e->buf_mem[1];
+    r.norm = e->norm;
+    r.ctrl = e->ctrl;
+    {
+      ProfScope ps(P_PRODUCT, double(B) * 5 * (M * Nh) * e->csize, st);
+      ce = ks->rows_product(2, r, unsigned(cdiv(r.nlines, 2 * ks->tiles.nlp2)), B, st);
+    }
+    if (ce != cudaSuccess) return cuda_fail(ce, "rhs pass 2 (2-D)");
+  }
+  if (first_stage) {
+    k_ctrl_dt<<<unsigned(cdiv(B, 128)), 128, 0, st>>>(e->ctrl, int(B), C, double(N), e->Md, e->prec);
+    ce = cudaGetLastError();
+    if (ce != cudaSuccess) return cuda_fail(ce, "k_ctrl_dt");
+  }
+  const char* bsrc;
+  long long b_row, b_comp, b_mem, ninner;
+  if (e->dim == 3) {
+    // pass 4: forward along y, keep retained rows: B1 -> B2 [6][M][N][Nh]
+    ColArgs a4{};
+    a4.in = e->buf[2];
+    a4.out = e->buf[0];
+    a4.tw = e->tw;
+    a4.ninner = Nh;
+    a4.ntile = int(cdiv(Nh, nc));
+    a4.n_short = int(N);
+    a4.in_row = Nh;
+    a4.out_row = Nh;
+    a4.in_outer = M * Nh;
+    a4.out_outer = N * Nh;
+    a4.in_comp = M * M * Nh;
+    a4.out_comp = M * N * Nh;
+    a4.in_mem = e->buf_mem[2];
+    a4.out_mem = e->buf_mem[0];
+    a4.ctrl = e->ctrl;
+    {
+      ProfScope ps(P_FWD_Y, double(B) * 6 * (M * M * Nh + M * N * Nh) * e->csize, st);
+      ce = ks->cols(COLK_TRUNC_FWD, a4, unsigned(a4.ntile * M), 6, B, st);
+    }
+    if (ce != cudaSuccess) return cuda_fail(ce, "rhs pass 4");
+    bsrc = e->buf[0];
+    b_row = N * Nh;
+    b_comp = M * N * Nh;
+    b_mem = e->buf_mem[0];
+    ninner = N * Nh;
+  } else {
+    bsrc = e->buf[1];
+    b_row = Nh;
+    b_comp = M * Nh;
+    b_mem = e->buf_mem[1];
+    ninner = Nh;
+  }
+  EpiArgs ep{};
+  ep.B = bsrc;
+  ep.u = u;
+  ep.u0 = u0 ? u0 : u;
+  ep.out = out;
+  ep.tw = e->tw;
+  ep.ninner = ninner;
+  const int ncm = e->dim == 3 ? ks->tiles.ncm3 : ks->tiles.ncm2;
+  ep.ntile = int(cdiv(ninner, ncm));
+  ep.N = int(N);
+  ep.nh = int(Nh);
+  ep.B_row = b_row;
+  ep.B_comp = b_comp;
+  ep.B_mem = b_mem;
+  ep.u_row = e->dim == 3 ? N * Nh : Nh;
+  ep.u_comp = e->dim == 3 ? N * N * Nh : N * Nh;
+  ep.u_mem = e->state_mem;
+  ep.mode = mode;
+  ep.visc = e->visc;
+  ep.ctrl = e->ctrl;
+  {
+    // B read + u read + out write (+ u0 read in stages 2 and 3)
+    const long long nb = e->dim == 3 ? 6 : 3;
+    const long long modes = e->dim == 3 ? N * N * Nh : N * Nh;
+    const double elems = double(nb) * M * ninner + double(e->dim) * modes * ((mode >= MODE_RK2) ? 3 : 2);
+    ProfScope ps(P_EPILOGUE, double(B) * elems * e->csize, st);
+    ce = ks->epilogue(e->dim, ep, unsigned(ep.ntile), B, st);
+  }
+  if (ce != cudaSuccess) return cuda_fail(ce, "rhs epilogue pass");
+  return AZ_OK;
+}
+
+}  // namespace azb
+
+az_status az_euler_dudt(az_euler e, void* dudt_hat, const void* u_hat, double t, double dt, double C,
+                        void* stream) {
+  (void)t;
+  (void)dt;
+  if (!e || !dudt_hat || !u_hat) return fail(AZ_ERR_INVALID, "az_euler_dudt: null argument");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // A plain right-hand side: clear any skip flag left by a finished simulation.
+  k_ctrl_begin_host<<<unsigned(cdiv(e->batch, 128)), 128, 0, st>>>(e->ctrl, e->batch, 0.0);
+  AZB_CUDA(cudaGetLastError());
+  return rhs(e, u_hat, nullptr, dudt_hat, MODE_DUDT, false, C, st);
+}
+
+az_status az_euler_dt(az_euler e, double C, void* stream, double* out) {
+  if (!e || !out) return fail(AZ_ERR_INVALID, "az_euler_dt: null argument");
+  std::vector<Ctrl> h(e->batch);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  AZB_CUDA(cudaMemcpyAsync(h.data(), e->ctrl, sizeof(Ctrl) * e->batch, cudaMemcpyDeviceToHost, st));
+  AZB_CUDA(cudaStreamSynchronize(st));
+  for (int b = 0; b < e->batch; ++b) {
+    double umax;
+    if (e->prec == 0) {
+      std::memcpy(&umax, &h[b].umax64, sizeof(double));
+    } else {
+      float f;
+      std::memcpy(&f, &h[b].umax32, sizeof(float));
+      umax = f;
+    }
+    const double u_max_ = umax / e->Md;
+    out[b] = C / ((double)e->N * u_max_);
+  }
+  for (int b = 0; b < e->batch; ++b)
+    if (h[b].err) return fail(AZ_ERR_NONFINITE, "non-finite value in the CFL reduction");
+  return AZ_OK;
+}
+
+az_status az_profile_enable(int on) {
+  g_prof = on != 0;
+  return AZ_OK;
+}
+
+az_status az_profile_read(double* ms, double* bytes, long long* launches, int npass) {
+  if (npass < P_NPASS) return fail(AZ_ERR_INVALID, "az_profile_read: need room for every pass");
+  for (int p = 0; p < npass; ++p) {
+    if (ms) ms[p] = 0;
+    if (bytes) bytes[p] = 0;
+    if (launches) launches[p] = 0;
+  }
+  for (auto& r : g_prof_recs) {
+    cudaError_t ce = cudaEventSynchronize(r.b);
+    if (ce != cudaSuccess) return cuda_fail(ce, "az_profile_read");
+    float t = 0;
+    cudaEventElapsedTime(&t, r.a, r.b);
+    if (ms) ms[r.pass] += t;
+    if (bytes) bytes[r.pass] += r.bytes;
+    if (launches) launches[r.pass] += 1;
+    g_prof_pool.push_back(r.a);
+    g_prof_pool.push_back(r.b);
+  }
+  g_prof_recs.clear();
+  return AZ_OK;
+}
+
+// ---------------------------------------------------------------------------
+// SSP-RK3
+// ---------------------------------------------------------------------------
+struct az_rk3_s {
+  az_euler eq;
+  void* u1 = nullptr;
+  void* u2 = nullptr;
+};
+
+az_status az_rk3_create(az_euler eq, az_rk3* out) {
+  if (!eq || !out) return fail(AZ_ERR_INVALID, "az_rk3_create: null argument");
+  auto* r = new az_rk3_s();
+  r->eq = eq;
+  const size_t bytes = size_t(eq->state_elems) * eq->csize;
+  if (cudaMalloc(&r->u1, bytes) != cudaSuccess || cudaMalloc(&r->u2, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(r->u1);
+    cudaFree(r->u2);
+    delete r;
+    return fail(AZ_ERR_NOMEM, "az_rk3_create: stage arrays");
+  }
+  *out = r;
+  return AZ_OK;
+}
+
+az_status az_rk3_destroy(az_rk3 r) {
+  if (!r) return AZ_OK;
+  cudaFree(r->u1);
+  cudaFree(r->u2);
+  delete r;
+  return AZ_OK;
+}
+
+namespace azb {
+// The three stages of SSP_RK3::integrate (ssp_rk3.hpp:48-64); the control
+// block must already hold max_dt and skip for this step.
+static az_status rk3_stages(az_rk3 r, void* u, double C, cudaStream_t st) {
+  az_euler e = r->eq;
+  az_status s;
+  s = rhs(e, u, nullptr, r->u1, MODE_RK1, true, C, st);
+  if (s != AZ_OK) return s;
+  s = rhs(e, r->u1, u, r->u2, MODE_RK2, false, C, st);
+  if (s != AZ_OK) return s;
+  return rhs(e, r->u2, u, u, MODE_RK3, false, C, st);
+}
+}  // namespace azb
+
+az_status az_rk3_integrate(az_rk3 r, double t, double max_dt, double C, void* u_hat, void* stream,
+                           double* dt_out) {
+  (void)t;
+  if (!r || !u_hat) return fail(AZ_ERR_INVALID, "az_rk3_integrate: null argument");
+  az_euler e = r->eq;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  k_ctrl_begin_host<<<unsigned(cdiv(e->batch, 128)), 128, 0, st>>>(e->ctrl, e->batch, max_dt);
+  AZB_CUDA(cudaGetLastError());
+  az_status s = rk3_stages(r, u_hat, C, st);
+  if (s != AZ_OK) return s;
+  std::vector<Ctrl> h(e->batch);
+  AZB_CUDA(cudaMemcpyAsync(h.data(), e->ctrl, sizeof(Ctrl) * e->batch, cudaMemcpyDeviceToHost, st));
+  AZB_CUDA(cudaStreamSynchronize(st));
+  for (int b = 0; b < e->batch; ++b) {
+    if (dt_out) dt_out[b] = h[b].dt;
+    if (h[b].err) return fail(AZ_ERR_NONFINITE, "non-finite value in the CFL reduction");
+  }
+  return AZ_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Simulation
+// ---------------------------------------------------------------------------
+struct az_sim_s {
+  az_rk3 ts;
+  double C;
+  void* u = nullptr;
+  Ctrl* host = nullptr;  // pinned mirror of the control blocks
+};
+
+az_status az_sim_create(az_rk3 ts, double C, const void* u_init, void* stream, az_sim* out) {
+  if (!ts || !u_init || !out) return fail(AZ_ERR_INVALID, "az_sim_create: null argument");
+  az_euler e = ts->eq;
+  auto* s = new az_sim_s();
+  s->ts = ts;
+  s->C = C;
+  const size_t bytes = size_t(e->state_elems) * e->csize;
+  if (cudaMalloc(&s->u, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    delete s;
+    return fail(AZ_ERR_NOMEM, "az_sim_create: state");
+  }
+  if (cudaMallocHost(&s->host, sizeof(Ctrl) * e->batch) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(s->u);
+    delete s;
+    return fail(AZ_ERR_NOMEM, "az_sim_create: pinned control mirror");
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaError_t ce = cudaMemcpyAsync(s->u, u_init, bytes, cudaMemcpyDeviceToDevice, st);
+  if (ce == cudaSuccess) ce = cudaMemsetAsync(e->ctrl, 0, sizeof(Ctrl) * e->batch, st);
+  if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+  if (ce != cudaSuccess) {
+    cudaFree(s->u);
+    cudaFreeHost(s->host);
+    delete s;
+    return cuda_fail(ce, "az_sim_create");
+  }
+  *out = s;
+  return AZ_OK;
+}
+
+az_status az_sim_destroy(az_sim s) {
+  if (!s) return AZ_OK;
+  cudaFree(s->u);
+  cudaFreeHost(s->host);
+  delete s;
+  return AZ_OK;
+}
+
+void* az_sim_u(az_sim s) { return s ? s->u : nullptr; }
+
+namespace azb {
+__global__ void k_ctrl_set_tend(Ctrl* c, int n, double t_end) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    c[i].t_end = t_end;
+    c[i].skip = 0;
+  }
+}
+__global__ void k_ctrl_finish(Ctrl* c, int n, double t_end) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    c[i].time = t_end;  // simulation.cpp:102
+    c[i].skip = 0;
+  }
+}
+
+static double visc_cap(az_euler e, double C) {
+  const double eps = e->eps_visc;
+  if (eps == 0.0) return INFINITY;
+  const double piN = 3.14159265358979323846 * (double)e->N;
+  return C * 2. / (eps * (piN * piN));  // simulation.cpp:92-93
+}
+
+static az_status sim_step(az_sim s, cudaStream_t st) {
+  az_euler e = s->ts->eq;
+  const unsigned g = unsigned(cdiv(e->batch, 128));
+  k_ctrl_begin_sim<<<g, 128, 0, st>>>(e->ctrl, e->batch, visc_cap(e, s->C));
+  AZB_CUDA(cudaGetLastError());
+  az_status r = rk3_stages(s->ts, s->u, s->C, st);
+  if (r != AZ_OK) return r;
+  k_ctrl_end<<<g, 128, 0, st>>>(e->ctrl, e->batch);
+  AZB_CUDA(cudaGetLastError());
+  return AZ_OK;
+}
+}  // namespace azb
+
+az_status az_sim_simulate_until(az_sim s, double t, void* stream) {
+  if (!s) return fail(AZ_ERR_INVALID, "az_sim_simulate_until: null argument");
+  az_euler e = s->ts->eq;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const unsigned g = unsigned(cdiv(e->batch, 128));
+  k_ctrl_set_tend<<<g, 128, 0, st>>>(e->ctrl, e->batch, t);
+  AZB_CUDA(cudaGetLastError());
+  int chunk = 1;
+  for (;;) {
+    for (int i = 0; i < chunk; ++i) {
+      az_status r = sim_step(s, st);
+      if (r != AZ_OK) return r;
+    }
+    AZB_CUDA(cudaMemcpyAsync(s->host, e->ctrl, sizeof(Ctrl) * e->batch, cudaMemcpyDeviceToHost, st));
+    AZB_CUDA(cudaStreamSynchronize(st));
+    // A member is done once its clock reached t (simulation.cpp:90).
+    double min_left = INFINITY;
+    bool any = false;
+    for (int b = 0; b < e->batch; ++b) {
+      if (s->host[b].err) return fail(AZ_ERR_NONFINITE, "non-finite value in the CFL reduction");
+      if (s->host[b].time < t) {
+        any = true;
+        const double dt = s->host[b].dt > 0 ? s->host[b].dt : 0.0;
+        const double left = dt > 0 ? (t - s->host[b].time) / dt : 1.0;
+        if (left < min_left) min_left = left;
+      }
+    }
+    if (!any) break;
+    // Steps that cannot overshoot any member's end (a finished member's
+    // steps are skipped on the device anyway).
+    chunk = int(std::floor(min_left * 0.9));
+    if (chunk < 1) chunk = 1;
+    if (chunk > 64) chunk = 64;
+  }
+  k_ctrl_finish<<<g, 128, 0, st>>>(e->ctrl, e->batch, t);
+  AZB_CUDA(cudaGetLastError());
+  return AZ_OK;
+}
+
+az_status az_sim_steps(az_sim s, int nsteps, void* stream) {
+  if (!s || nsteps < 0) return fail(AZ_ERR_INVALID, "az_sim_steps: bad argument");
+  az_euler e = s->ts->eq;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const unsigned g = unsigned(cdiv(e->batch, 128));
+  k_ctrl_set_tend<<<g, 128, 0, st>>>(e->ctrl, e->batch, INFINITY);
+  AZB_CUDA(cudaGetLastError());
+  for (int i = 0; i < nsteps; ++i) {
+    az_status r = sim_step(s, st);
+    if (r != AZ_OK) return r;
+  }
+  return AZ_OK;
+}
+
+az_status az_sim_state(az_sim s, void* stream, double* time, long long* nsteps, double* dt) {
+  if (!s) return fail(AZ_ERR_INVALID, "az_sim_state: null argument");
+  az_euler e = s->ts->eq;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  AZB_CUDA(cudaMemcpyAsync(s->host, e->ctrl, sizeof(Ctrl) * e->batch, cudaMemcpyDeviceToHost, st));
+  AZB_CUDA(cudaStreamSynchronize(st));
+  for (int b = 0; b < e->batch; ++b) {
+    if (time) time[b] = s->host[b].time;
+    if (nsteps) nsteps[b] = s->host[b].nsteps;
+    if (dt) dt[b] = s->host[b].dt;
+  }
+  return AZ_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Control kernels
+// ---------------------------------------------------------------------------
+namespace azb {
+__global__ void k_ctrl_begin_host(Ctrl* c, int n, double max_dt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    c[i].skip = 0;
+    c[i].max_dt = max_dt;
+    c[i].err = 0;
+  }
+}
+__global__ void k_ctrl_begin_sim(Ctrl* c, int n, double cap) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    if (!(c[i].time < c[i].t_end)) {
+      c[i].skip = 1;
+    } else {
+      c[i].skip = 0;
+      c[i].max_dt = fmin(c[i].t_end - c[i].time, cap);
+    }
+  }
+}
+__global__ void k_ctrl_clear_max(Ctrl* c, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    c[i].umax64 = 0ull;
+    c[i].umax32 = 0u;
+  }
+}
+__global__ void k_ctrl_dt(Ctrl* c, int n, double C, double Nphys, double Md, int fp32) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && !c[i].skip) {
+    const double m = fp32 ? (double)__uint_as_float(c[i].umax32) : __longlong_as_double((long long)c[i].umax64);
+    const double u_max_ = m / Md;
+    const double dtc = C / (Nphys * u_max_);
+    c[i].dt = fmin(dtc, c[i].max_dt);
+  }
+}
+__global__ void k_ctrl_end(Ctrl* c, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && !c[i].skip) {
+    c[i].time += c[i].dt;
+    c[i].nsteps += 1;
+  }
+}
+}  // namespace azb
+
+// ---------------------------------------------------------------------------
+// FFT<Dim>
+// ---------------------------------------------------------------------------
+struct az_fft_s {
+  int dim, prec, direction, nt;
+  long long n_vars;
+  long long shape[3];
+  long long nh;
+  const KernelSet* ks[3] = {nullptr, nullptr, nullptr};
+  const void* tw[3] = {nullptr, nullptr, nullptr};
+  void* u_hat;
+  void* u;
+  void* work = nullptr;
+  size_t work_bytes = 0;
+  size_t csize;
+};
+
+az_status az_fft_create(const az_fft_desc* d, void* u_hat, void* u, az_fft* out) {
+  if (!d || !out || !u_hat || !u) return fail(AZ_ERR_INVALID, "az_fft_create: null argument");
+  *out = nullptr;
+  if (d->dim < 1 || d->dim > 3) return fail(AZ_ERR_INVALID, "az_fft_create: dim must be 1, 2 or 3");
+  if (d->transform_last < 1 || d->transform_last > d->dim)
+    return fail(AZ_ERR_INVALID, "az_fft_create: transform_last must be in [1, dim]");
+  if (d->n_vars < 1) return fail(AZ_ERR_INVALID, "az_fft_create: n_vars must be >= 1");
+  if (d->precision != AZ_PREC_F64 && d->precision != AZ_PREC_F32)
+    return fail(AZ_ERR_INVALID, "az_fft_create: unknown precision");
+  auto* f = new az_fft_s();
+  f->dim = d->dim;
+  f->prec = d->precision;
+  f->direction = d->direction;
+  f->nt = d->transform_last;
+  f->n_vars = d->n_vars;
+  f->u_hat = u_hat;
+  f->u = u;
+  f->csize = d->precision == 0 ? 16 : 8;
+  for (int a = 0; a < d->dim; ++a) {
+    f->shape[a] = d->shape[a];
+    const bool transformed = a >= d->dim - d->transform_last;
+    if (!transformed) continue;
+    const KernelSet* ks = kernel_set(d->precision, int(d->shape[a]));
+    if (!ks || d->shape[a] < 4) {
+      delete f;
+      return fail(AZ_ERR_UNSUPPORTED,
+                  "az_fft_create: length " + std::to_string(d->shape[a]) + " has no compiled transform");
+    }
+    f->ks[a] = ks;
+    az_status s = twiddles(d->precision, int(d->shape[a]), &f->tw[a]);
+    if (s != AZ_OK) {
+      delete f;
+      return s;
+    }
+  }
+  f->nh = d->shape[d->dim - 1] / 2 + 1;
+  long long celems = f->n_vars * f->nh;
+  for (int a = 0; a < d->dim - 1; ++a) celems *= d->shape[a];
+  if (f->nt > 1) {
+    f->work_bytes = size_t(celems) * f->csize;
+    if (cudaMalloc(&f->work, f->work_bytes) != cudaSuccess) {
+      cudaGetLastError();
+      delete f;
+      return fail(AZ_ERR_NOMEM, "az_fft_create: work area");
+    }
+  }
+  *out = f;
+  return AZ_OK;
+}
+
+az_status az_fft_destroy(az_fft f) {
+  if (!f) return AZ_OK;
+  cudaFree(f->work);
+  delete f;
+  return AZ_OK;
+}
+
+size_t az_fft_work_area_size(az_fft f) { return f ? f->work_bytes : 0; }
+
+namespace azb {
+// Column transform of the complex array [n_vars][n0..][nh] along axis `ax`.
+static az_status fft_axis(az_fft f, int ax, const void* in, void* out, int kind, cudaStream_t st) {
+  const KernelSet* ks = f->ks[ax];
+  const long long rows = f->shape[ax];
+  long long inner = f->nh;
+  for (int a = ax + 1; a < f->dim - 1; ++a) inner *= f->shape[a];
+  long long outer = f->n_vars;
+  for (int a = 0; a < ax; ++a) outer *= f->shape[a];
+  ColArgs c{};
+  c.in = in;
+  c.out = out;
+  c.tw = f->tw[ax];
+  c.ninner = inner;
+  c.ntile = int(cdiv(inner, ks->tiles.nc));
+  c.n_short = int(rows);
+  c.in_row = inner;
+  c.out_row = inner;
+  c.in_outer = rows * inner;
+  c.out_outer = rows * inner;
+  c.ctrl = nullptr;
+  // grid.y carries the outer index in slices of at most 65535
+  long long done = 0;
+  while (done < outer) {
+    const long long chunk = outer - done > 65535 ? 65535 : outer - done;
+    ColArgs cc = c;
+    cc.in = static_cast<const char*>(in) + done * rows * inner * f->csize;
+    cc.out = static_cast<char*>(out) + done * rows * inner * f->csize;
+    cc.in_comp = rows * inner;
+    cc.out_comp = rows * inner;
+    cc.in_outer = 0;
+    cc.out_outer = 0;
+    cudaError_t ce = ks->cols(kind, cc, unsigned(cc.ntile), unsigned(chunk), 1, st);
+    if (ce != cudaSuccess) return cuda_fail(ce, "fft column pass");
+    done += chunk;
+  }
+  return AZ_OK;
+}
+}  // namespace azb
+
+az_status az_fft_forward(az_fft f, void* stream) {
+  if (!f) return fail(AZ_ERR_INVALID, "az_fft_forward: null argument");
+  if (!(f->direction & AZ_FFT_FORWARD)) return fail(AZ_ERR_INVALID, "FFT was not planned for forward transforms");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int last = f->dim - 1;
+  long long lines = f->n_vars;
+  for (int a = 0; a < last; ++a) lines *= f->shape[a];
+  RealRowArgs r{};
+  r.in = f->u;
+  r.out = f->u_hat;
+  r.tw = f->tw[last];
+  r.nlines = lines;
+  r.in_line = f->shape[last];
+  r.out_line = f->nh;
+  cudaError_t ce = f->ks[last]->r2c(r, unsigned(cdiv(lines, 2 * f->ks[last]->tiles.nlpr)), st);
+  if (ce != cudaSuccess) return cuda_fail(ce, "fft r2c pass");
+  for (int ax = last - 1; ax >= f->dim - f->nt; --ax) {
+    az_status s = fft_axis(f, ax, f->u_hat, f->u_hat, COLK_PLAIN_FWD, st);
+    if (s != AZ_OK) return s;
+  }
+  return AZ_OK;
+}
+
+az_status az_fft_backward(az_fft f, void* stream) {
+  if (!f) return fail(AZ_ERR_INVALID, "az_fft_backward: null argument");
+  if (!(f->direction & AZ_FFT_BACKWARD)) return fail(AZ_ERR_INVALID, "FFT was not planned for backward transforms");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int last = f->dim - 1;
+  const void* src = f->u_hat;
+  for (int ax = f->dim - f->nt; ax < last; ++ax) {
+    az_status s = fft_axis(f, ax, src, f->work, COLK_PLAIN_INV, st);
+    if (s != AZ_OK) return s;
+    src = f->work;
+  }
+  long long lines = f->n_vars;
+  for (int a = 0; a < last; ++a) lines *= f->shape[a];
+  RealRowArgs r{};
+  r.in = src;
+  r.out = f->u;
+  r.tw = f->tw[last];
+  r.nlines = lines;
+  r.in_line = f->nh;
+  r.out_line = f->shape[last];
+  cudaError_t ce = f->ks[last]->c2r(r, unsigned(cdiv(lines, 2 * f->ks[last]->tiles.nlpr)), st);
+  if (ce != cudaSuccess) return cuda_fail(ce, "fft c2r pass");
+  return AZ_OK;
+}

@@ -1,0 +1,375 @@
+#!/usr/bin/env python
+"""Benchmark of the Euler hot path: 3-D 256^3 Taylor-Green SSP-RK3 member-steps/s.
+
+Workload (config "TG-3D 256^3"): u = (sin x cos y cos z, -cos x sin y cos z, 0)
+sampled at x_i = 2 pi i / N, N = 256 (padded M = 384), SmoothCutoff viscosity
+eps = 0.05 (eps_N = 0.05/N, k0 = 2 pi sqrt(N)), SSP-RK3, C = 0.2.  A step is
+one SSP-RK3 step (three right-hand sides) of every member of the batch.
+
+  value   batched FP32-bulk member-steps/s, state resident in HBM, timed with
+          CUDA events over K steps (max over ranks); every step reads inputs
+          larger than L2 (126 MB), so no flush is needed.
+  e2e     the same metric through the public API (SSP_RK3.integrate) with host
+          buffers: each step copies the batch state host->device from pinned
+          memory, steps, and copies the new state back.
+  fp64_*  the plain FP64 form, one member, same workload.
+
+``--impl reference`` times the CPU restatement of the reference's path (the
+oracle; the reference itself cannot be built here) on the host cores.
+Multi-GPU: replicas only (ensemble members are independent; weak scaling).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "3D 256^3 Euler member-steps/s, batched FP32 vs plain FP64 at L2<=1e-5; p99 latency"
+UNIT = "member-steps/s"
+VISC_CFG = {"type": "Smooth Cutoff", "eps": 0.05}
+C_CFL = 0.2
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--batch", type=int, default=4)
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel_key):
+    """DRAM bytes per launch of a kernel from the committed ncu summary, or None."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f).get(kernel_key)
+    except Exception:
+        return None
+
+
+def cpu_sample(n, cores):
+    """One right-hand side of one member with the oracle (FP64, scipy.fft on
+    `cores` threads); returns (seconds, member-steps in the sample)."""
+    from oracle import euler_oracle as ora
+    ora.set_workers(cores)
+    g = ora.Grid(3, n)
+    eq = ora.IncompressibleEuler(g, ora.make_viscosity(VISC_CFG, g))
+    u = ora.initialize(ora.taylor_green_workload(3, n))
+    t0 = time.perf_counter()
+    eq.dudt(u)
+    return time.perf_counter() - t0, 1.0 / 3.0
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    cores = os.cpu_count() or 1
+    samples = []
+    for i in range(args.warmup + args.steps):
+        sec, ms = cpu_sample(args.n, cores)
+        if i >= args.warmup:
+            samples.append(sec / ms)
+    per_member_step = statistics.mean(samples)
+    value = 1.0 / per_member_step
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_member_step * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"TG-3D {args.n}^3, M={3 * args.n // 2}, SmoothCutoff eps=0.05, SSP-RK3, C=0.2",
+                   "members": 1, "l2": "inputs larger than L2"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"one right-hand side of one {args.n}^3 member per step (1/3 member-step), "
+                                   "numpy/scipy.fft restatement of the reference CPU path"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local):
+    import numpy as np
+    import torch
+
+    import azeban_b200 as az
+    from azeban_b200 import _lib
+    from azeban_b200 import init as azinit
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    N, B, K, W = args.n, args.batch, args.steps, args.warmup
+    g = az.Grid(3, N)
+    visc = az.make_viscosity(VISC_CFG, g)
+    stream = torch.cuda.current_stream()
+
+    # ---- FP32-bulk batched form (the headline) ---------------------------
+    u0_32 = azinit.taylor_green(3, N, "f32")
+    batch_u = u0_32.unsqueeze(0).repeat(B, 1, 1, 1, 1).contiguous()
+    eq32 = az.IncompressibleEuler(g, visc, "f32", batch=B)
+    ts32 = az.SSP_RK3(eq32)
+    sim32 = az.Simulation(g, C_CFL, ts32, batch_u)
+    sim32.steps(W)
+    torch.cuda.synchronize()
+
+    sampler = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    time.sleep(0.3)
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(K + 1)]
+    evs[0].record(stream)
+    for i in range(K):
+        sim32.steps(1)
+        evs[i + 1].record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    barrier()
+    step_ms = [evs[i].elapsed_time(evs[i + 1]) for i in range(K)]
+    total_ms = max_over_ranks(evs[0].elapsed_time(evs[K]))
+    value = world * B * K / (total_ms / 1e3)
+    ms_per_step = total_ms / K
+    sorted_ms = sorted(step_ms)
+    p50 = sorted_ms[len(sorted_ms) // 2]
+    p99 = sorted_ms[min(len(sorted_ms) - 1, math.ceil(0.99 * len(sorted_ms)) - 1)]
+
+    # ---- live per-pass roofline over K more steps --------------------------
+    _lib.lib.az_profile_enable(1)
+    sim32.steps(K)
+    torch.cuda.synchronize()
+    _lib.lib.az_profile_enable(0)
+    import ctypes as ct
+    ms = (ct.c_double * 5)()
+    by = (ct.c_double * 5)()
+    nl = (ct.c_longlong * 5)()
+    _lib.check(_lib.lib.az_profile_read(ms, by, nl, 5))
+    pass_names = ["inv_x_pad", "inv_y_pad", "z_product", "fwd_y_trunc", "fwd_x_epilogue"]
+    kernel_keys = ["k_cols_pad_inv_x", "k_cols_pad_inv_y", "k_rows_product", "k_cols_trunc_fwd",
+                   "k_fwd_epilogue"]
+    peak, peak_kind = measured_peak_hbm()
+    passes = {}
+    for i, nm in enumerate(pass_names):
+        if nl[i]:
+            avg_ms = ms[i] / nl[i]
+            passes[nm] = {"launches": nl[i], "avg_ms": avg_ms, "bytes_per_launch": by[i] / nl[i],
+                          "gbs": by[i] / nl[i] / (avg_ms * 1e-3) / 1e9,
+                          "share": ms[i] / max(sum(ms), 1e-30)}
+    dom = max(range(5), key=lambda i: ms[i])
+    dom_bytes = by[dom] / max(nl[dom], 1)
+    dom_ms = ms[dom] / max(nl[dom], 1)
+    achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
+    traffic = ncu_traffic(kernel_keys[dom])
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic, "kernel": pass_names[dom],
+                "peak_source": peak_kind, "passes": passes,
+                "step_bytes_model_gb": sum(by) / K / 1e9,
+                "step_gbs_model": sum(by) / K / (ms_per_step * 1e-3) / 1e9}
+
+    # ---- plain FP64 form, one member ----------------------------------------
+    fp64 = None
+    if not args.no_fp64:
+        u0_64 = azinit.taylor_green(3, N, "f64")
+        eq64 = az.IncompressibleEuler(g, visc, "f64")
+        sim64 = az.Simulation(g, C_CFL, az.SSP_RK3(eq64), u0_64)
+        sim64.steps(W)
+        K64 = max(3, K // 2)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sim64.steps(K64)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t64 = max_over_ranks(e0.elapsed_time(e1))
+        fp64 = {"member_steps_per_s": world * K64 / (t64 / 1e3), "ms_per_step": t64 / K64, "steps": K64}
+        del sim64, eq64
+
+    # ---- accuracy: FP32 bulk vs FP64 at t = 1 (one member) ----------------
+    accuracy = None
+    if not args.no_accuracy:
+        eqa = az.IncompressibleEuler(g, visc, "f32")
+        eqb = az.IncompressibleEuler(g, visc, "f64")
+        sa = az.Simulation(g, C_CFL, az.SSP_RK3(eqa), azinit.taylor_green(3, N, "f32"))
+        sb = az.Simulation(g, C_CFL, az.SSP_RK3(eqb), azinit.taylor_green(3, N, "f64"))
+        sa.simulate_until(1.0)
+        sb.simulate_until(1.0)
+        a = sa.u().to(torch.complex128)
+        b = sb.u()
+        accuracy = {"t": 1.0, "l2_rel_fp32_vs_fp64": float(torch.linalg.vector_norm(a - b) /
+                                                          torch.linalg.vector_norm(b)),
+                    "steps_fp32": sa.state()[1][0], "steps_fp64": sb.state()[1][0]}
+        del sa, sb, eqa, eqb
+
+    # ---- end to end through the public API with host buffers ---------------
+    e2e = None
+    if not args.no_e2e:
+        host_in = batch_u.cpu().pin_memory()
+        host_out = torch.empty_like(host_in).pin_memory()
+        dev_u = torch.empty_like(batch_u)
+        cap = C_CFL * 2.0 / (visc.eps * (math.pi * N) ** 2)
+        for _ in range(max(1, W // 2)):
+            dev_u.copy_(host_in, non_blocking=True)
+            ts32.integrate(0.0, cap, C_CFL, dev_u)
+            host_out.copy_(dev_u, non_blocking=True)
+        torch.cuda.synchronize()
+        barrier()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        for _ in range(K):
+            dev_u.copy_(host_in, non_blocking=True)
+            ts32.integrate(0.0, cap, C_CFL, dev_u)
+            host_out.copy_(dev_u, non_blocking=True)
+        a1.record(stream)
+        torch.cuda.synchronize()
+        te = max_over_ranks(a0.elapsed_time(a1))
+        nbytes = host_in.numel() * host_in.element_size()
+        e2e = {"value": world * B * K / (te / 1e3), "unit": UNIT, "h2d_bytes_per_step": nbytes,
+               "d2h_bytes_per_step": nbytes + 8 * B}
+
+    # ---- CPU baseline (rank 0, N = 1) ---------------------------------------
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cores = os.cpu_count() or 1
+        sec, msteps = cpu_sample(N, cores)
+        cpu = {"value": msteps / sec, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"one right-hand side of one {N}^3 member (1/3 member-step), FP64 numpy/scipy.fft "
+                         f"restatement of the reference CPU path, {sec:.1f} s"}
+
+    launches_per_step = 1 + 3 * 5 + 1 + 1
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"TG-3D {N}^3 batched FP32 bulk, M={3 * N // 2}, SmoothCutoff eps=0.05, "
+                                   f"SSP-RK3, C=0.2", "members_per_gpu": B, "N": N, "M": 3 * N // 2,
+                       "precision": "fp32 bulk, fp64 CFL", "l2": "inputs larger than L2 (no flush)",
+                       "parallelism": f"replicas x{world}"},
+            "p50_step_ms": p50, "p99_step_ms": p99,
+            "fp64": fp64,
+            "fp32_over_fp64": (value / world) / fp64["member_steps_per_s"] * world if fp64 else None,
+            "accuracy": accuracy,
+            "e2e": e2e,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+            "gpu_launches": launches_per_step * K,
+        }
+        if fp64:
+            line["fp32_over_fp64"] = (value / world) / (fp64["member_steps_per_s"] / world)
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    run_ours(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

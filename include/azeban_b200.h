@@ -1,0 +1,182 @@
+/*
+ * azeban_b200 -- C ABI of the B200-native spectral-viscosity incompressible
+ * Euler right-hand side, its SSP-RK3 stepper and its real FFTs.
+ *
+ * Every entry point returns az_status (AZ_OK == 0) and never exits the
+ * process; az_last_error_string() describes the last failure of the calling
+ * thread.  Array arguments are DEVICE pointers in the layouts of the
+ * reference (row-major, spectral arrays [n_vars][N][(N)][N/2+1] complex,
+ * r2c along the last axis; include/azeban/grid.hpp:89-99).  Complex values
+ * are interleaved (re, im) pairs of the solve's precision.  Streams are
+ * cudaStream_t passed as void* (NULL = legacy default stream).
+ *
+ * Each declaration names the reference interface it replaces (paths relative
+ * to the reference project root).
+ */
+#ifndef AZEBAN_B200_H_
+#define AZEBAN_B200_H_
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  AZ_OK = 0,
+  AZ_ERR_INVALID = 1,     /* bad argument (shape, null pointer, key) */
+  AZ_ERR_UNSUPPORTED = 2, /* a size with no compiled transform length */
+  AZ_ERR_CUDA = 3,        /* a CUDA runtime call failed */
+  AZ_ERR_NOMEM = 4,       /* device allocation failed */
+  AZ_ERR_NONFINITE = 5    /* the CFL reduction met Inf or NaN */
+} az_status;
+
+typedef enum { AZ_PREC_F64 = 0, AZ_PREC_F32 = 1 } az_precision;
+
+typedef enum {
+  AZ_VISC_NONE = 0,          /* NoViscosity, spectral_viscosity.hpp:125-128 */
+  AZ_VISC_SMOOTH_CUTOFF = 1, /* SmoothCutoff1D, spectral_viscosity.hpp:56-77 */
+  AZ_VISC_STEP = 2,          /* Step1D, spectral_viscosity.hpp:40-54 */
+  AZ_VISC_QUADRATIC = 3      /* Quadratic, spectral_viscosity.hpp:103-123 */
+} az_visc_type;
+
+/* Viscosity as the reference's factory leaves it: eps already divided by
+ * N^{2s-1} and k0 = m0 N^theta (spectral_viscosity_factory.hpp:29-89). */
+typedef struct {
+  int type;        /* az_visc_type */
+  double eps;
+  double s;        /* SmoothCutoff / Step */
+  double k0;       /* SmoothCutoff / Step */
+  long long N;     /* Quadratic */
+} az_visc;
+
+/* Replaces Grid<Dim> + the IncompressibleEuler<Dim, Visc, NoForcing>
+ * constructor (include/azeban/grid.hpp:30-53,
+ * include/azeban/equations/incompressible_euler.hpp:56-96). */
+typedef struct {
+  int dim;               /* 2 or 3 */
+  long long N_phys;      /* N, even */
+  long long N_phys_pad;  /* M >= N, a supported transform length */
+  int precision;         /* az_precision; AZ_PREC_F32 = FP32 bulk, FP64 CFL */
+  az_visc visc;
+  int batch;             /* ensemble members of this N, >= 1; arrays are [batch][d][...] */
+} az_euler_desc;
+
+typedef struct az_euler_s* az_euler;
+typedef struct az_rk3_s* az_rk3;
+typedef struct az_sim_s* az_sim;
+typedef struct az_fft_s* az_fft;
+
+/* Last error of the calling thread ("" if none). */
+const char* az_last_error_string(void);
+
+/* Transform lengths with compiled kernels, written to out[0..*n) (capacity cap). */
+az_status az_supported_lengths(int* out, int cap, int* n);
+
+/* ---- Equation<Dim> (include/azeban/equations/equation.hpp:27-56) -------- */
+
+/* IncompressibleEuler ctor; allocates its workspace
+ * (incompressible_euler.hpp:56-96, src/azeban/memory/workspace.cpp:41-69). */
+az_status az_euler_create(const az_euler_desc* desc, az_euler* out);
+az_status az_euler_destroy(az_euler eq);
+
+/* Equation<Dim>::dudt (incompressible_euler.hpp:103-120): dudt_hat <- RHS(u_hat).
+ * dudt_hat may equal u_hat.  t, dt, C are accepted for interface parity
+ * (they only feed forcing, which this path does not have). */
+az_status az_euler_dudt(az_euler eq, void* dudt_hat, const void* u_hat, double t, double dt,
+                        double C, void* stream);
+
+/* Equation<Dim>::dt (incompressible_euler.hpp:122-124): C / (N u_max) of the
+ * last dudt, per member (out[batch]).  Synchronises the stream. */
+az_status az_euler_dt(az_euler eq, double C, void* stream, double* out);
+
+/* Equation<Dim>::n_vars / visc (equation.hpp:44-46). */
+int az_euler_n_vars(az_euler eq);
+double az_euler_visc(az_euler eq);
+
+/* Bytes of device workspace the equation holds. */
+size_t az_euler_workspace_size(az_euler eq);
+
+/* ---- TimeIntegrator<Dim> / SSP_RK3<Dim> (include/azeban/evolution/time_integrator.hpp:30-60,
+ *      include/azeban/evolution/ssp_rk3.hpp:28-76) ---------------------- */
+
+/* SSP_RK3 ctor: allocates the stage arrays u1, u2 (ssp_rk3.hpp:39-42). */
+az_status az_rk3_create(az_euler eq, az_rk3* out);
+az_status az_rk3_destroy(az_rk3 ts);
+
+/* SSP_RK3::integrate (ssp_rk3.hpp:48-64): one step of every member in place;
+ * dt = min(equation dt(C), max_dt) of each member is written to dt_out[batch]
+ * (host memory).  Synchronises the stream. */
+az_status az_rk3_integrate(az_rk3 ts, double t, double max_dt, double C, void* u_hat,
+                           void* stream, double* dt_out);
+
+/* ---- Simulation<Dim> (include/azeban/simulation.hpp:30-93, src/azeban/simulation.cpp:89-102) */
+
+/* Simulation ctor from an initial state (copied into the simulation). */
+az_status az_sim_create(az_rk3 ts, double C, const void* u_hat_init, void* stream, az_sim* out);
+az_status az_sim_destroy(az_sim sim);
+
+/* Simulation::simulate_until: each member steps with its own dt until its
+ * clock reaches t; the step size and the clock stay on the device. */
+az_status az_sim_simulate_until(az_sim sim, double t, void* stream);
+
+/* Exactly nsteps SSP-RK3 steps of every member (max_dt = viscous cap), with
+ * no host synchronisation: the timed unit of the benchmark. */
+az_status az_sim_steps(az_sim sim, int nsteps, void* stream);
+
+/* Device pointer of the state [batch][d][...] (Simulation::u()). */
+void* az_sim_u(az_sim sim);
+
+/* Per-member clock, step count and last dt (host arrays of length batch).
+ * Any pointer may be NULL.  Synchronises the stream. */
+az_status az_sim_state(az_sim sim, void* stream, double* time, long long* nsteps, double* dt);
+
+/* ---- FFT<Dim> (include/azeban/operations/fft.hpp:37-121,
+ *      make_fft src/azeban/operations/fft_factory.cpp:10-48) ----------- */
+
+enum { AZ_FFT_FORWARD = 1, AZ_FFT_BACKWARD = 2 }; /* fft.hpp:28 */
+
+typedef struct {
+  int dim;                 /* 1, 2 or 3 */
+  long long n_vars;        /* data_dim_: transforms batched over the first axis */
+  long long shape[3];      /* real-space extents of the dim axes */
+  int transform_last;      /* number of trailing axes transformed (1..dim) */
+  int precision;           /* az_precision */
+  int direction;           /* AZ_FFT_FORWARD | AZ_FFT_BACKWARD */
+} az_fft_desc;
+
+/* make_fft + FFT::initialize(u_hat, u): binds the arrays and allocates the
+ * work area. */
+az_status az_fft_create(const az_fft_desc* desc, void* u_hat, void* u, az_fft* out);
+az_status az_fft_destroy(az_fft fft);
+/* FFT::forward: u_hat <- unnormalised r2c(u) (fft.hpp:95). */
+az_status az_fft_forward(az_fft fft, void* stream);
+/* FFT::backward: u <- unnormalised c2r(u_hat) (fft.hpp:96); u_hat is kept. */
+az_status az_fft_backward(az_fft fft, void* stream);
+/* FFT::get_work_area_size (fft.hpp:93). */
+size_t az_fft_work_area_size(az_fft fft);
+
+/* ---- per-pass timing (no reference counterpart; replaces the reference's
+ *      Profiler, include/azeban/profiler.hpp:35-135, for the transform passes) */
+
+/* When on, every pass launch of a right-hand side is bracketed by two CUDA
+ * events on its stream. */
+az_status az_profile_enable(int on);
+/* Sums per pass id (0 inverse x, 1 inverse y, 2 product, 3 forward y,
+ * 4 forward x + projection + stage) of event-timed milliseconds, algorithmic
+ * bytes (one read of every input and one write of every output) and launch
+ * counts since the last read; npass >= 5.  Waits for the recorded events. */
+az_status az_profile_read(double* ms, double* bytes, long long* launches, int npass);
+
+/* ---- leray (src/azeban/operations/leray.cpp:28-116) --------------------- */
+
+/* In-place projection of u_hat [batch][dim][N]([N])[N/2+1] onto divergence-free
+ * fields; the |k| = 0 mode is set to zero.  Used when building initial data
+ * (include/azeban/init/initializer.hpp:68-75). */
+az_status az_leray(int dim, long long N, int precision, void* u_hat, int batch, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AZEBAN_B200_H_ */
