@@ -3,17 +3,20 @@
 //
 // One 3-D right-hand side (reference: IncompressibleEuler::dudt,
 // include/azeban/equations/incompressible_euler.hpp:103-120) runs as five
-// passes, each one HBM read and one HBM write of the live array:
-//   1 k_cols<PAD,  inverse>  along x: u_hat [3][N][N][Nh] -> A1 [3][M][N][Nh]
+// passes, each one HBM read and one HBM write of the live array.  The
+// intermediates keep the component index innermost, so a tile of consecutive
+// columns is one contiguous run per row in every pass:
+//   1 k_cols<PAD,  inverse>  along x: u_hat [3][N][N][Nh] -> A1 [M][N][Nh][3]
 //                            (copy_to_padded along x fused into the loads)
-//   2 k_cols<PAD,  inverse>  along y: A1 -> A2 [3][M][M][Nh]
+//   2 k_cols<PAD,  inverse>  along y: A1 -> A2 [M][M][Nh][3]
 //   3 k_rows_product         along z: c2r, max|u|, B = u (x) u, r2c, keep
-//                            k < Nh: A2 -> B1 [6][M][M][Nh]
-//   4 k_cols<TRUNC, forward> along y, keep the N retained rows: B1 -> B2 [6][M][N][Nh]
+//                            k < Nh: A2 -> B1 [M][M][Nh][6]
+//   4 k_cols<TRUNC, forward> along y, keep the N retained rows: B1 -> B2 [M][N][Nh][6]
 //   5 k_fwd_epilogue         along x, keep retained rows, then computeDudt
 //                            (Leray projection of i k.B, spectral viscosity)
 //                            and the SSP-RK3 stage combination: B2 + u -> out
-// 2-D uses passes 1 (along x), 3 (along y) and 5.
+// 2-D uses passes 1 (along x), 3 (along y) and 5, with A1 [M][Nh][2] and
+// B1 [M][Nh][3].
 #pragma once
 
 #include "az_types.h"
@@ -53,6 +56,8 @@ struct ColArgs {
   long long in_mem, out_mem;
   Ctrl* ctrl;     // optional: per-member skip flags
   int clear_max;  // nonzero: also reset the member's CFL accumulator
+  int in_ci;      // input component interleave: column p reads component p % in_ci
+                  // at in_comp stride, position p / in_ci (1: plain columns)
 };
 
 // Batched column transforms along a strided axis.  grid = (ntile * nouter,
@@ -80,8 +85,8 @@ __global__ void __launch_bounds__(NC * Plan<L>::TPL) k_cols(ColArgs a) {
   const int tl = threadIdx.x / NC;
   const long long p = (long long)tile * NC + col;
   const bool valid = p < a.ninner;
-  const C* in = reinterpret_cast<const C*>(a.in) + member * a.in_mem + comp * a.in_comp +
-                outer * a.in_outer + p;
+  const long long pin = a.in_ci == 1 ? comp * a.in_comp + p : (p % a.in_ci) * a.in_comp + p / a.in_ci;
+  const C* in = reinterpret_cast<const C*>(a.in) + member * a.in_mem + outer * a.in_outer + pin;
   C* out = reinterpret_cast<C*>(a.out) + member * a.out_mem + comp * a.out_comp +
            outer * a.out_outer + p;
   load_twiddles<C, L>(tw, reinterpret_cast<const C*>(a.tw));
@@ -102,13 +107,12 @@ __global__ void __launch_bounds__(NC * Plan<L>::TPL) k_cols(ColArgs a) {
 }
 
 struct RowArgs {
-  const void* in;
-  void* out;
+  const void* in;   // lines of nh x DIM complex, component innermost
+  void* out;        // lines of nh x NB complex, component innermost
   const void* tw;
   long long nlines;  // lines per member
-  int nh;            // complex entries per spectral line (N/2+1)
+  int nh;            // spectral bins per line (N/2+1)
   long long in_line, out_line;
-  long long in_comp, out_comp;
   long long in_mem, out_mem;
   double norm;  // 1 / (N^{d/2} M^{d/2})
   Ctrl* ctrl;
@@ -123,15 +127,16 @@ template <> __device__ __forceinline__ void atomic_max_abs<float>(Ctrl* c, float
 }
 
 // Hermitian extension of a half spectrum: bin m of the length-L spectrum of a
-// real signal whose bins [0, nh) are stored at `line` (nullptr: all zero).
-// The imaginary parts of bin 0 and of bin L/2 are dropped, as a c2r does.
+// real signal whose bins [0, nh) are stored at line[bin * stride] (nullptr:
+// all zero).  The imaginary parts of bin 0 and of bin L/2 are dropped, as a
+// c2r does.
 template <typename C, int L>
-__device__ __forceinline__ C herm_bin(const C* line, int nh, int m) {
+__device__ __forceinline__ C herm_bin(const C* line, int nh, int m, int stride = 1) {
   using T = decltype(C::x);
   const bool mirror = m > L / 2;
   const int mm = mirror ? L - m : m;
   C v = cmk<C>(T(0), T(0));
-  if (line != nullptr && mm < nh) v = line[mm];
+  if (line != nullptr && mm < nh) v = line[mm * stride];
   if (mirror) v.y = -v.y;
   if (m == 0 || 2 * m == L) v.y = T(0);
   return v;
@@ -177,8 +182,8 @@ __global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NLP * Plan<L>::TPL)
     for (int h = 0; h < 2; ++h) {
       const int s = 2 * q + h;
       const long long ln = line0 + 2 * p + s / DIM;
-      const C* src = ln < a.nlines ? in + (s % DIM) * a.in_comp + ln * a.in_line : nullptr;
-      x[h] = herm_bin<C, L>(src, a.nh, m);
+      const C* src = ln < a.nlines ? in + ln * a.in_line + (s % DIM) : nullptr;
+      x[h] = herm_bin<C, L>(src, a.nh, m, DIM);
     }
     sm[m * SROW + cz] = cmk<C>(x[0].x - x[1].y, x[0].y + x[1].x);
   }
@@ -261,19 +266,22 @@ __global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NLP * Plan<L>::TPL)
   }
   __syncthreads();
 
-  // 5. Separate the two real spectra and write bins [0, nh).
-  for (int idx = tid; idx < NFWD * a.nh; idx += NT) {
-    const int k = idx % a.nh;
-    const int cf = idx / a.nh;
-    const int p = cf / NB;
-    const int c = cf % NB;
+  // 5. Separate the two real spectra and write bins [0, nh), component
+  //    fastest so the stores of a line are contiguous.
+  const int per_pair = NB * a.nh;
+  for (int idx = tid; idx < NLP * per_pair; idx += NT) {
+    const int p = idx / per_pair;
+    const int r = idx - p * per_pair;
+    const int k = r / NB;
+    const int c = r - k * NB;
+    const int cf = p * NB + c;
     const C fk = sm[k * SROW + cf];
     const C fm = sm[((L - k) % L) * SROW + cf];
     const C xa = cmk<C>(T(0.5) * (fk.x + fm.x), T(0.5) * (fk.y - fm.y));
     const C xb = cmk<C>(T(0.5) * (fk.y + fm.y), T(-0.5) * (fk.x - fm.x));
     const long long la = line0 + 2 * p;
-    if (la < a.nlines) out[c * a.out_comp + la * a.out_line + k] = xa;
-    if (la + 1 < a.nlines) out[c * a.out_comp + (la + 1) * a.out_line + k] = xb;
+    if (la < a.nlines) out[la * a.out_line + r] = xa;
+    if (la + 1 < a.nlines) out[(la + 1) * a.out_line + r] = xb;
   }
 
   // CFL reduction: warp, then block, then one atomic per CTA.
@@ -298,7 +306,7 @@ __global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NLP * Plan<L>::TPL)
 }
 
 struct EpiArgs {
-  const void* B;
+  const void* B;  // [M][modes][NB], component innermost
   const void* u;
   const void* u0;
   void* out;
@@ -306,7 +314,7 @@ struct EpiArgs {
   long long ninner;  // modes per retained row: N*Nh (3-D) or Nh (2-D)
   int ntile;
   int N, nh;
-  long long B_row, B_comp, B_mem;
+  long long B_row, B_mem;
   long long u_row, u_comp, u_mem;
   int mode;
   Visc visc;
@@ -372,13 +380,13 @@ __global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NCM * Plan<L>::TPL)
   load_twiddles<C, L>(tw, reinterpret_cast<const C*>(a.tw));
   __syncthreads();
   {
+    // column col = (mode pl, component c) with c fastest: one contiguous run
     const int col = tid % NC;
     const int tl = tid / NC;
-    const int c = col / NCM;
-    const int pl = col % NCM;
+    const int pl = col / NB;
     const long long p = (long long)tile * NCM + pl;
     const bool valid = p < a.ninner;
-    const C* Bp = reinterpret_cast<const C*>(a.B) + member * a.B_mem + c * a.B_comp + p;
+    const C* Bp = reinterpret_cast<const C*>(a.B) + member * a.B_mem + (long long)tile * NC + col;
     fft_columns<C, -1, L, SROW, true>(
         sm, tw, col, tl,
         [&](int m) -> C { return valid ? Bp[m * a.B_row] : cmk<C>(T(0), T(0)); },
@@ -403,7 +411,7 @@ __global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NCM * Plan<L>::TPL)
     const int i_ = i >= N / 2 + 1 ? i - N : i;
     C Bv[NB];
 #pragma unroll
-    for (int c = 0; c < NB; ++c) Bv[c] = sm[i * SROW + c * NCM + pl];
+    for (int c = 0; c < NB; ++c) Bv[c] = sm[i * SROW + pl * NB + c];
     const long long off = (long long)i * a.u_row + p;
     C uv[DIM];
 #pragma unroll

@@ -220,15 +220,15 @@ az_status az_euler_create(const az_euler_desc* d, az_euler* out) {
   e->csize = d->precision == 0 ? 16 : 8;
   const long long N = e->N, M = e->M, Nh = e->Nh;
   if (e->dim == 3) {
-    e->buf_mem[0] = 6 * M * N * Nh;  // A1 [3][M][N][Nh] then B2 [6][M][N][Nh]
-    e->buf_mem[1] = 3 * M * M * Nh;  // A2
-    e->buf_mem[2] = 6 * M * M * Nh;  // B1
+    e->buf_mem[0] = 6 * M * N * Nh;  // A1 [M][N][Nh][3], later B2 [M][N][Nh][6]
+    e->buf_mem[1] = 3 * M * M * Nh;  // A2 [M][M][Nh][3]
+    e->buf_mem[2] = 6 * M * M * Nh;  // B1 [M][M][Nh][6]
     e->state_mem = 3 * N * N * Nh;
     e->norm = 1.0 / (std::pow(std::sqrt((double)N), 3) * std::pow(std::sqrt((double)M), 3));
     e->Md = (double)(M * M * M);
   } else {
-    e->buf_mem[0] = 2 * M * Nh;  // A1
-    e->buf_mem[1] = 3 * M * Nh;  // B1
+    e->buf_mem[0] = 2 * M * Nh;  // A1 [M][Nh][2]
+    e->buf_mem[1] = 3 * M * Nh;  // B1 [M][Nh][3]
     e->buf_mem[2] = 0;
     e->state_mem = 2 * N * Nh;
     e->norm = 1.0 / (std::pow(std::sqrt((double)N), 2) * std::pow(std::sqrt((double)M), 2));
@@ -298,60 +298,57 @@ static az_status rhs(az_euler e, const void* u, const void* u0, void* out, int m
   const int nc = ks->tiles.nc;
   cudaError_t ce;
   if (e->dim == 3) {
-    // pass 1: inverse along x with padding, state -> A1 [3][M][N][Nh]
+    // pass 1: inverse along x with padding, state [3][N][N][Nh] -> A1 [M][N][Nh][3]
     ColArgs a1{};
     a1.in = u;
     a1.out = e->buf[0];
     a1.tw = e->tw;
-    a1.ninner = N * Nh;
+    a1.ninner = 3 * N * Nh;
     a1.ntile = int(cdiv(a1.ninner, nc));
     a1.n_short = int(N);
     a1.in_row = N * Nh;
-    a1.out_row = N * Nh;
+    a1.out_row = 3 * N * Nh;
     a1.in_comp = N * N * Nh;
-    a1.out_comp = M * N * Nh;
+    a1.in_ci = 3;
     a1.in_mem = e->state_mem;
     a1.out_mem = e->buf_mem[0];
     a1.ctrl = e->ctrl;
     a1.clear_max = 1;
     {
       ProfScope ps(P_INV_X, double(B) * 3 * (N * N * Nh + M * N * Nh) * e->csize, st);
-      ce = ks->cols(COLK_PAD_INV, a1, unsigned(a1.ntile), 3, B, st);
+      ce = ks->cols(COLK_PAD_INV, a1, unsigned(a1.ntile), 1, B, st);
     }
     if (ce != cudaSuccess) return cuda_fail(ce, "rhs pass 1");
-    // pass 2: inverse along y with padding, A1 -> A2 [3][M][M][Nh]
+    // pass 2: inverse along y with padding, A1 -> A2 [M][M][Nh][3]
     ColArgs a2{};
     a2.in = e->buf[0];
     a2.out = e->buf[1];
     a2.tw = e->tw;
-    a2.ninner = Nh;
-    a2.ntile = int(cdiv(Nh, nc));
+    a2.ninner = 3 * Nh;
+    a2.ntile = int(cdiv(a2.ninner, nc));
     a2.n_short = int(N);
-    a2.in_row = Nh;
-    a2.out_row = Nh;
-    a2.in_outer = N * Nh;
-    a2.out_outer = M * Nh;
-    a2.in_comp = M * N * Nh;
-    a2.out_comp = M * M * Nh;
+    a2.in_row = 3 * Nh;
+    a2.out_row = 3 * Nh;
+    a2.in_outer = N * 3 * Nh;
+    a2.out_outer = M * 3 * Nh;
+    a2.in_ci = 1;
     a2.in_mem = e->buf_mem[0];
     a2.out_mem = e->buf_mem[1];
     a2.ctrl = e->ctrl;
     {
       ProfScope ps(P_INV_Y, double(B) * 3 * (M * N * Nh + M * M * Nh) * e->csize, st);
-      ce = ks->cols(COLK_PAD_INV, a2, unsigned(a2.ntile * M), 3, B, st);
+      ce = ks->cols(COLK_PAD_INV, a2, unsigned(a2.ntile * M), 1, B, st);
     }
     if (ce != cudaSuccess) return cuda_fail(ce, "rhs pass 2");
-    // pass 3: z lines, product, CFL max: A2 -> B1 [6][M][M][Nh]
+    // pass 3: z lines, product, CFL max: A2 -> B1 [M][M][Nh][6]
     RowArgs r{};
     r.in = e->buf[1];
     r.out = e->buf[2];
     r.tw = e->tw;
     r.nlines = M * M;
     r.nh = int(Nh);
-    r.in_line = Nh;
-    r.out_line = Nh;
-    r.in_comp = M * M * Nh;
-    r.out_comp = M * M * Nh;
+    r.in_line = 3 * Nh;
+    r.out_line = 6 * Nh;
     r.in_mem = e->buf_mem[1];
     r.out_mem = e->buf_mem[2];
     r.norm = e->norm;
@@ -362,36 +359,36 @@ static az_status rhs(az_euler e, const void* u, const void* u0, void* out, int m
     }
     if (ce != cudaSuccess) return cuda_fail(ce, "rhs pass 3");
   } else {
+    // pass 1: inverse along x with padding, state [2][N][Nh] -> A1 [M][Nh][2]
     ColArgs a1{};
     a1.in = u;
     a1.out = e->buf[0];
     a1.tw = e->tw;
-    a1.ninner = Nh;
-    a1.ntile = int(cdiv(Nh, nc));
+    a1.ninner = 2 * Nh;
+    a1.ntile = int(cdiv(a1.ninner, nc));
     a1.n_short = int(N);
     a1.in_row = Nh;
-    a1.out_row = Nh;
+    a1.out_row = 2 * Nh;
     a1.in_comp = N * Nh;
-    a1.out_comp = M * Nh;
+    a1.in_ci = 2;
     a1.in_mem = e->state_mem;
     a1.out_mem = e->buf_mem[0];
     a1.ctrl = e->ctrl;
     a1.clear_max = 1;
     {
       ProfScope ps(P_INV_X, double(B) * 2 * (N * Nh + M * Nh) * e->csize, st);
-      ce = ks->cols(COLK_PAD_INV, a1, unsigned(a1.ntile), 2, B, st);
+      ce = ks->cols(COLK_PAD_INV, a1, unsigned(a1.ntile), 1, B, st);
     }
     if (ce != cudaSuccess) return cuda_fail(ce, "rhs pass 1 (2-D)");
+    // pass 2: y lines, product, CFL max: A1 -> B1 [M][Nh][3]
     RowArgs r{};
     r.in = e->buf[0];
     r.out = e->buf[1];
     r.tw = e->tw;
     r.nlines = M;
     r.nh = int(Nh);
-    r.in_line = Nh;
-    r.out_line = Nh;
-    r.in_comp = M * Nh;
-    r.out_comp = M * Nh;
+    r.in_line = 2 * Nh;
+    r.out_line = 3 * Nh;
     r.in_mem = e->buf_mem[0];
     r.out_mem = e->buf_mem[1];
     r.norm = e->norm;
@@ -408,39 +405,36 @@ static az_status rhs(az_euler e, const void* u, const void* u0, void* out, int m
     if (ce != cudaSuccess) return cuda_fail(ce, "k_ctrl_dt");
   }
   const char* bsrc;
-  long long b_row, b_comp, b_mem, ninner;
+  long long b_row, b_mem, ninner;
   if (e->dim == 3) {
-    // pass 4: forward along y, keep retained rows: B1 -> B2 [6][M][N][Nh]
+    // pass 4: forward along y, keep retained rows: B1 -> B2 [M][N][Nh][6]
     ColArgs a4{};
     a4.in = e->buf[2];
     a4.out = e->buf[0];
     a4.tw = e->tw;
-    a4.ninner = Nh;
-    a4.ntile = int(cdiv(Nh, nc));
+    a4.ninner = 6 * Nh;
+    a4.ntile = int(cdiv(a4.ninner, nc));
     a4.n_short = int(N);
-    a4.in_row = Nh;
-    a4.out_row = Nh;
-    a4.in_outer = M * Nh;
-    a4.out_outer = N * Nh;
-    a4.in_comp = M * M * Nh;
-    a4.out_comp = M * N * Nh;
+    a4.in_row = 6 * Nh;
+    a4.out_row = 6 * Nh;
+    a4.in_outer = M * 6 * Nh;
+    a4.out_outer = N * 6 * Nh;
+    a4.in_ci = 1;
     a4.in_mem = e->buf_mem[2];
     a4.out_mem = e->buf_mem[0];
     a4.ctrl = e->ctrl;
     {
       ProfScope ps(P_FWD_Y, double(B) * 6 * (M * M * Nh + M * N * Nh) * e->csize, st);
-      ce = ks->cols(COLK_TRUNC_FWD, a4, unsigned(a4.ntile * M), 6, B, st);
+      ce = ks->cols(COLK_TRUNC_FWD, a4, unsigned(a4.ntile * M), 1, B, st);
     }
     if (ce != cudaSuccess) return cuda_fail(ce, "rhs pass 4");
     bsrc = e->buf[0];
-    b_row = N * Nh;
-    b_comp = M * N * Nh;
+    b_row = 6 * N * Nh;
     b_mem = e->buf_mem[0];
     ninner = N * Nh;
   } else {
     bsrc = e->buf[1];
-    b_row = Nh;
-    b_comp = M * Nh;
+    b_row = 3 * Nh;
     b_mem = e->buf_mem[1];
     ninner = Nh;
   }
@@ -456,7 +450,6 @@ static az_status rhs(az_euler e, const void* u, const void* u0, void* out, int m
   ep.N = int(N);
   ep.nh = int(Nh);
   ep.B_row = b_row;
-  ep.B_comp = b_comp;
   ep.B_mem = b_mem;
   ep.u_row = e->dim == 3 ? N * Nh : Nh;
   ep.u_comp = e->dim == 3 ? N * N * Nh : N * Nh;
@@ -907,6 +900,7 @@ static az_status fft_axis(az_fft f, int ax, const void* in, void* out, int kind,
   c.in_outer = rows * inner;
   c.out_outer = rows * inner;
   c.ctrl = nullptr;
+  c.in_ci = 1;
   // grid.y carries the outer index in slices of at most 65535
   long long done = 0;
   while (done < outer) {
