@@ -16,6 +16,7 @@ AZ_OK = 0
 AZ_PREC_F64, AZ_PREC_F32 = 0, 1
 AZ_VISC_NONE, AZ_VISC_SMOOTH_CUTOFF, AZ_VISC_STEP, AZ_VISC_QUADRATIC = 0, 1, 2, 3
 AZ_FFT_FORWARD, AZ_FFT_BACKWARD = 1, 2
+AZ_NOALLOC_SCRATCH_BYTES = 64 * 1024 * 1024
 
 STATUS_NAMES = {0: "AZ_OK", 1: "AZ_ERR_INVALID", 2: "AZ_ERR_UNSUPPORTED", 3: "AZ_ERR_CUDA",
                 4: "AZ_ERR_NOMEM", 5: "AZ_ERR_NONFINITE"}
@@ -29,7 +30,7 @@ EXPORTS = [
     "az_sim_create", "az_sim_destroy", "az_sim_simulate_until", "az_sim_steps", "az_sim_u",
     "az_sim_state",
     "az_fft_create", "az_fft_destroy", "az_fft_forward", "az_fft_backward", "az_fft_work_area_size",
-    "az_leray", "az_profile_enable", "az_profile_read",
+    "az_leray", "az_profile_enable", "az_profile_read", "az_euler_dudt_noalloc",
 ]
 
 
@@ -90,6 +91,7 @@ def _load():
         "az_leray": (I, [I, LL, I, P, I, P]),
         "az_profile_enable": (I, [I]),
         "az_profile_read": (I, [ct.POINTER(D), ct.POINTER(D), ct.POINTER(LL), I]),
+        "az_euler_dudt_noalloc": (I, [I, LL, LL, I, ct.POINTER(az_visc), P, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

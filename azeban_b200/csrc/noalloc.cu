@@ -1,0 +1,154 @@
+// The right-hand side without any allocation by the library.
+//
+// Some callers cannot let a library allocate device memory: a host code that
+// owns every device allocation through its own pool or arena (a cudaMalloc
+// from inside the library bypasses its accounting, or fails under its memory
+// cap), or a run whose device memory is fixed at start-up.  For them,
+// az_euler_dudt_noalloc takes its scratch from one file-scope device array of
+// AZ_NOALLOC_SCRATCH_BYTES instead of a workspace; the caller passes the
+// input and output arrays as usual.
+//
+// The array is a static __device__ variable: every GPU that loads the library
+// holds it until the process exits.  Host code cannot use its name as a device
+// address, so the first call on each device (with that device current) looks
+// the address up with cudaGetSymbolAddress and keeps it; make that first call
+// before any stream capture.  All calls share the one array and it keeps the
+// last call's contents, so each call rewrites everything it reads (control
+// block, twiddle table) before use.  Calls whose work overlaps on the GPU
+// (other streams, other host threads) race on the array.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <mutex>
+#include <string>
+
+#include "runtime_internal.h"
+
+namespace azb {
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[AZ_NOALLOC_SCRATCH_BYTES];
+
+static std::mutex g_noalloc_mutex;
+static void* g_noalloc_ptr[64] = {};
+
+// Device address of g_noalloc_scratch on the current device.
+static az_status noalloc_scratch(void** out) {
+  int dev = 0;
+  cudaError_t ce = cudaGetDevice(&dev);
+  if (ce != cudaSuccess) return set_error(AZ_ERR_CUDA, cudaGetErrorString(ce));
+  if (dev < 0 || dev >= 64) return set_error(AZ_ERR_UNSUPPORTED, "az_euler_dudt_noalloc: device index >= 64");
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (g_noalloc_ptr[dev] == nullptr) {
+    void* p = nullptr;
+    ce = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (ce != cudaSuccess)
+      return set_error(AZ_ERR_CUDA, (std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(ce)).c_str());
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return AZ_OK;
+}
+
+// W_L^m = exp(-2 pi i m / L) for m in [0, L), from sincospi in FP64.
+template <typename T>
+__global__ void k_noalloc_twiddles(cvec<T>* tw, int L) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m < L) {
+    double s, c;
+    sincospi(-2.0 * double(m) / double(L), &s, &c);
+    tw[m] = cmk<cvec<T>>(T(c), T(s));
+  }
+}
+
+static size_t round256(size_t b) { return (b + 255) / 256 * 256; }
+
+}  // namespace azb
+
+using namespace azb;
+
+az_status az_euler_dudt_noalloc(int dim, long long N_phys, long long N_phys_pad, int precision,
+                                const az_visc* visc, void* dudt_hat, const void* u_hat, void* stream) {
+  if (!visc || !dudt_hat || !u_hat) return set_error(AZ_ERR_INVALID, "az_euler_dudt_noalloc: null argument");
+  if (dim != 2 && dim != 3)
+    return set_error(AZ_ERR_INVALID, "Incompressible Euler is only implemented for 2D and 3D");
+  if (N_phys < 2 || (N_phys % 2) != 0) return set_error(AZ_ERR_INVALID, "N_phys must be even and >= 2");
+  if (N_phys_pad < N_phys) return set_error(AZ_ERR_INVALID, "N_phys_pad must be >= N_phys");
+  if (precision != AZ_PREC_F64 && precision != AZ_PREC_F32) return set_error(AZ_ERR_INVALID, "unknown precision");
+  if (visc->type < 0 || visc->type > 3) return set_error(AZ_ERR_INVALID, "unknown viscosity type");
+  const KernelSet* ks = find_kernel_set(precision, int(N_phys_pad));
+  if (!ks) return set_error(AZ_ERR_UNSUPPORTED, "N_phys_pad has no compiled transform length");
+
+  az_euler_s e;
+  e.dim = dim;
+  e.prec = precision;
+  e.batch = 1;
+  e.N = N_phys;
+  e.M = N_phys_pad;
+  e.Nh = e.N / 2 + 1;
+  e.visc.type = visc->type;
+  e.visc.eps = visc->eps;
+  e.visc.s = visc->s;
+  e.visc.k0 = visc->k0;
+  e.visc.N = visc->N;
+  e.eps_visc = visc->type == AZ_VISC_NONE ? 0.0 : visc->eps;
+  e.ks = ks;
+  e.csize = precision == AZ_PREC_F64 ? 16 : 8;
+  e.prof = false;
+  const long long N = e.N, M = e.M, Nh = e.Nh;
+  if (dim == 3) {
+    e.buf_mem[0] = 6 * M * N * Nh;
+    e.buf_mem[1] = 3 * M * M * Nh;
+    e.buf_mem[2] = 6 * M * M * Nh;
+    e.state_mem = 3 * N * N * Nh;
+    e.norm = 1.0 / (std::pow(std::sqrt((double)N), 3) * std::pow(std::sqrt((double)M), 3));
+    e.Md = (double)(M * M * M);
+  } else {
+    e.buf_mem[0] = 2 * M * Nh;
+    e.buf_mem[1] = 3 * M * Nh;
+    e.buf_mem[2] = 0;
+    e.state_mem = 2 * N * Nh;
+    e.norm = 1.0 / (std::pow(std::sqrt((double)N), 2) * std::pow(std::sqrt((double)M), 2));
+    e.Md = (double)(M * M);
+  }
+  e.state_elems = e.state_mem;
+
+  // Scratch layout: control block | twiddle table | buf0 | buf1 | buf2.
+  const size_t ctrl_bytes = round256(sizeof(Ctrl));
+  const size_t tw_bytes = round256(size_t(M) * e.csize);
+  size_t need = ctrl_bytes + tw_bytes;
+  size_t off[3];
+  for (int b = 0; b < 3; ++b) {
+    off[b] = need;
+    need += round256(size_t(e.buf_mem[b]) * e.csize);
+  }
+  if (need > size_t(AZ_NOALLOC_SCRATCH_BYTES)) {
+    const std::string msg = "az_euler_dudt_noalloc: this size needs " + std::to_string(need) +
+                            " bytes of scratch, above the fixed " +
+                            std::to_string((long long)AZ_NOALLOC_SCRATCH_BYTES) +
+                            " bytes; use az_euler_create / az_euler_dudt";
+    return set_error(AZ_ERR_UNSUPPORTED, msg.c_str());
+  }
+  void* base = nullptr;
+  az_status st = noalloc_scratch(&base);
+  if (st != AZ_OK) return st;
+  char* b = static_cast<char*>(base);
+  e.ctrl = reinterpret_cast<Ctrl*>(b);
+  e.tw = b + ctrl_bytes;
+  e.work = b;
+  e.work_bytes = need;
+  for (int i = 0; i < 3; ++i) e.buf[i] = b + off[i];
+
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // The array keeps the previous call's contents: rewrite the control block
+  // and the twiddle table of this call's length before the passes read them.
+  cudaError_t ce = cudaMemsetAsync(e.ctrl, 0, sizeof(Ctrl), s);
+  if (ce != cudaSuccess) return set_error(AZ_ERR_CUDA, cudaGetErrorString(ce));
+  const unsigned g = unsigned((M + 255) / 256);
+  if (precision == AZ_PREC_F64)
+    k_noalloc_twiddles<double><<<g, 256, 0, s>>>(reinterpret_cast<double2*>(b + ctrl_bytes), int(M));
+  else
+    k_noalloc_twiddles<float><<<g, 256, 0, s>>>(reinterpret_cast<float2*>(b + ctrl_bytes), int(M));
+  ce = cudaGetLastError();
+  if (ce != cudaSuccess) return set_error(AZ_ERR_CUDA, cudaGetErrorString(ce));
+  return euler_dudt_launch(&e, dudt_hat, u_hat, s);
+}

@@ -14,6 +14,7 @@
 #include "../../include/azeban_b200.h"
 #include "az_types.h"
 #include "kernel_set.cuh"
+#include "runtime_internal.h"
 
 namespace azb {
 
@@ -138,14 +139,14 @@ struct ProfScope {
   double bytes;
   cudaStream_t st;
   cudaEvent_t a = nullptr;
-  ProfScope(int p, double by, cudaStream_t s) : pass(p), bytes(by), st(s) {
-    if (g_prof) {
+  ProfScope(int p, double by, cudaStream_t s, bool allowed = true) : pass(p), bytes(by), st(s) {
+    if (g_prof && allowed) {
       a = prof_event();
       cudaEventRecord(a, st);
     }
   }
   ~ProfScope() {
-    if (g_prof && a) {
+    if (a) {
       cudaEvent_t b = prof_event();
       cudaEventRecord(b, st);
       g_prof_recs.push_back({pass, bytes, a, b});
@@ -160,26 +161,6 @@ using namespace azb;
 // ---------------------------------------------------------------------------
 // Equation
 // ---------------------------------------------------------------------------
-struct az_euler_s {
-  int dim, prec, batch;
-  long long N, M, Nh;
-  Visc visc;
-  double eps_visc;  // Equation::visc()
-  const KernelSet* ks;
-  const void* tw;
-  size_t csize;  // bytes per complex element
-  // workspace: buf0 [6][M][N][Nh] (3-D) | [2][M][Nh] (2-D), buf1, buf2
-  void* work = nullptr;
-  size_t work_bytes = 0;
-  char* buf[3] = {nullptr, nullptr, nullptr};
-  long long buf_mem[3] = {0, 0, 0};  // member strides (elements)
-  long long state_mem;               // member stride of a state array
-  long long state_elems;             // batch * state_mem
-  Ctrl* ctrl = nullptr;              // [batch]
-  double norm;
-  double Md;
-};
-
 const char* az_last_error_string(void) { return g_err.c_str(); }
 
 az_status az_supported_lengths(int* out, int cap, int* n) {
@@ -315,7 +296,7 @@ static az_status rhs(az_euler e, const void* u, const void* u0, void* out, int m
     a1.ctrl = e->ctrl;
     a1.clear_max = 1;
     {
-      ProfScope ps(P_INV_X, double(B) * 3 * (N * N * Nh + M * N * Nh) * e->csize, st);
+      ProfScope ps(P_INV_X, double(B) * 3 * (N * N * Nh + M * N * Nh) * e->csize, st, e->prof);
       ce = ks->cols(COLK_PAD_INV, a1, unsigned(a1.ntile), 1, B, st);
     }
     if (ce != cudaSuccess) return cuda_fail(ce, "rhs pass 1");
@@ -336,7 +317,7 @@ static az_status rhs(az_euler e, const void* u, const void* u0, void* out, int m
     a2.out_mem = e->buf_mem[1];
     a2.ctrl = e->ctrl;
     {
-      ProfScope ps(P_INV_Y, double(B) * 3 * (M * N * Nh + M * M * Nh) * e->csize, st);
+      ProfScope ps(P_INV_Y, double(B) * 3 * (M * N * Nh + M * M * Nh) * e->csize, st, e->prof);
       ce = ks->cols(COLK_PAD_INV, a2, unsigned(a2.ntile * M), 1, B, st);
     }
     if (ce != cudaSuccess) return cuda_fail(ce, "rhs pass 2");
@@ -354,7 +335,7 @@ static az_status rhs(az_euler e, const void* u, const void* u0, void* out, int m
     r.norm = e->norm;
     r.ctrl = e->ctrl;
     {
-      ProfScope ps(P_PRODUCT, double(B) * 9 * (M * M * Nh) * e->csize, st);
+      ProfScope ps(P_PRODUCT, double(B) * 9 * (M * M * Nh) * e->csize, st, e->prof);
       ce = ks->rows_product(3, r, unsigned(cdiv(r.nlines, 2 * ks->tiles.nlp3)), B, st);
     }
     if (ce != cudaSuccess) return cuda_fail(ce, "rhs pass 3");
@@ -376,7 +357,7 @@ static az_status rhs(az_euler e, const void* u, const void* u0, void* out, int m
     a1.ctrl = e->ctrl;
     a1.clear_max = 1;
     {
-      ProfScope ps(P_INV_X, double(B) * 2 * (N * Nh + M * Nh) * e->csize, st);
+      ProfScope ps(P_INV_X, double(B) * 2 * (N * Nh + M * Nh) * e->csize, st, e->prof);
       ce = ks->cols(COLK_PAD_INV, a1, unsigned(a1.ntile), 1, B, st);
     }
     if (ce != cudaSuccess) return cuda_fail(ce, "rhs pass 1 (2-D)");
@@ -394,7 +375,7 @@ static az_status rhs(az_euler e, const void* u, const void* u0, void* out, int m
     r.norm = e->norm;
     r.ctrl = e->ctrl;
     {
-      ProfScope ps(P_PRODUCT, double(B) * 5 * (M * Nh) * e->csize, st);
+      ProfScope ps(P_PRODUCT, double(B) * 5 * (M * Nh) * e->csize, st, e->prof);
       ce = ks->rows_product(2, r, unsigned(cdiv(r.nlines, 2 * ks->tiles.nlp2)), B, st);
     }
     if (ce != cudaSuccess) return cuda_fail(ce, "rhs pass 2 (2-D)");
@@ -424,7 +405,7 @@ static az_status rhs(az_euler e, const void* u, const void* u0, void* out, int m
     a4.out_mem = e->buf_mem[0];
     a4.ctrl = e->ctrl;
     {
-      ProfScope ps(P_FWD_Y, double(B) * 6 * (M * M * Nh + M * N * Nh) * e->csize, st);
+      ProfScope ps(P_FWD_Y, double(B) * 6 * (M * M * Nh + M * N * Nh) * e->csize, st, e->prof);
       ce = ks->cols(COLK_TRUNC_FWD, a4, unsigned(a4.ntile * M), 1, B, st);
     }
     if (ce != cudaSuccess) return cuda_fail(ce, "rhs pass 4");
@@ -462,7 +443,7 @@ static az_status rhs(az_euler e, const void* u, const void* u0, void* out, int m
     const long long nb = e->dim == 3 ? 6 : 3;
     const long long modes = e->dim == 3 ? N * N * Nh : N * Nh;
     const double elems = double(nb) * M * ninner + double(e->dim) * modes * ((mode >= MODE_RK2) ? 3 : 2);
-    ProfScope ps(P_EPILOGUE, double(B) * elems * e->csize, st);
+    ProfScope ps(P_EPILOGUE, double(B) * elems * e->csize, st, e->prof);
     ce = ks->epilogue(e->dim, ep, unsigned(ep.ntile), B, st);
   }
   if (ce != cudaSuccess) return cuda_fail(ce, "rhs epilogue pass");
@@ -482,6 +463,16 @@ az_status az_euler_dudt(az_euler e, void* dudt_hat, const void* u_hat, double t,
   AZB_CUDA(cudaGetLastError());
   return rhs(e, u_hat, nullptr, dudt_hat, MODE_DUDT, false, C, st);
 }
+
+namespace azb {
+az_status euler_dudt_launch(az_euler e, void* dudt_hat, const void* u_hat, cudaStream_t st) {
+  k_ctrl_begin_host<<<unsigned(cdiv(e->batch, 128)), 128, 0, st>>>(e->ctrl, e->batch, 0.0);
+  AZB_CUDA(cudaGetLastError());
+  return rhs(e, u_hat, nullptr, dudt_hat, MODE_DUDT, false, 0.0, st);
+}
+az_status set_error(az_status st, const char* msg) { return fail(st, msg); }
+const KernelSet* find_kernel_set(int precision, int L) { return kernel_set(precision, L); }
+}  // namespace azb
 
 az_status az_euler_dt(az_euler e, double C, void* stream, double* out) {
   if (!e || !out) return fail(AZ_ERR_INVALID, "az_euler_dt: null argument");

@@ -1,0 +1,41 @@
+// Internal to the library: the equation descriptor shared by the runtime
+// units (runtime.cu, noalloc.cu).
+#pragma once
+
+#include <cstddef>
+
+#include "../../include/azeban_b200.h"
+#include "az_types.h"
+#include "kernel_set.cuh"
+
+struct az_euler_s {
+  int dim, prec, batch;
+  long long N, M, Nh;
+  azb::Visc visc;
+  double eps_visc;  // Equation::visc()
+  const azb::KernelSet* ks;
+  const void* tw;
+  size_t csize;  // bytes per complex element
+  // workspace: buf0 [6][M][N][Nh] (3-D) | [2][M][Nh] (2-D), buf1, buf2
+  void* work = nullptr;
+  size_t work_bytes = 0;
+  char* buf[3] = {nullptr, nullptr, nullptr};
+  long long buf_mem[3] = {0, 0, 0};  // member strides (elements)
+  long long state_mem;               // member stride of a state array
+  long long state_elems;             // batch * state_mem
+  azb::Ctrl* ctrl = nullptr;              // [batch]
+  double norm;
+  double Md;
+  bool prof = true;  // false: never record per-pass timing events
+};
+
+
+namespace azb {
+// One right-hand side of every member of `e` (MODE_DUDT), the launch sequence
+// of az_euler_dudt: resets the members' skip flags, then runs the passes.
+az_status euler_dudt_launch(az_euler e, void* dudt_hat, const void* u_hat, cudaStream_t st);
+// Sets the thread's last-error string and returns st.
+az_status set_error(az_status st, const char* msg);
+// Compiled kernels of one (precision, transform length), or nullptr.
+const KernelSet* find_kernel_set(int precision, int L);
+}  // namespace azb

@@ -175,6 +175,25 @@ az_status az_profile_read(double* ms, double* bytes, long long* launches, int np
  * (include/azeban/init/initializer.hpp:68-75). */
 az_status az_leray(int dim, long long N, int precision, void* u_hat, int batch, void* stream);
 
+/* ---- right-hand side without allocation (no counterpart in the reference) */
+
+/* Size of the one device array that az_euler_dudt_noalloc takes its scratch from. */
+#define AZ_NOALLOC_SCRATCH_BYTES (64LL * 1024 * 1024)
+
+/* One right-hand side of one solve, the work of az_euler_dudt with batch 1,
+ * that allocates nothing: no cudaMalloc, no cudaFree, no allocating library
+ * call.  It has no counterpart in the reference.  It is for callers that
+ * cannot let a library allocate device memory, such as a host code that owns
+ * all device memory through its own pool under a fixed cap.  The scratch is
+ * one file-scope device array of AZ_NOALLOC_SCRATCH_BYTES, held by every GPU
+ * that loads the library until the process exits.  That bounds the sizes: at
+ * 3/2 padding, 3-D up to N = 64 and 2-D up to N = 1024, in either precision;
+ * a larger size returns AZ_ERR_UNSUPPORTED.  The first call on a device looks
+ * up the array's device address; make it before any stream capture.  Every
+ * call shares the array, so calls that overlap on the GPU race. */
+az_status az_euler_dudt_noalloc(int dim, long long N_phys, long long N_phys_pad, int precision,
+                                const az_visc* visc, void* dudt_hat, const void* u_hat, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
