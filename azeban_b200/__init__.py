@@ -6,12 +6,16 @@ reached through its C ABI (include/azeban_b200.h).
 """
 
 from ._lib import AzebanError, supported_lengths
-from .core import (FFT, FFT_BACKWARD, FFT_FORWARD, Grid, IncompressibleEuler, NoViscosity,
+from .core import (FFT, FFT_BACKWARD, FFT_FORWARD, Grid, Group, IncompressibleEuler, NoViscosity,
                    Quadratic, Simulation, SmoothCutoff1D, SSP_RK3, Step1D, leray, make_fft,
                    make_grid, make_viscosity, next_good_size, precision_code)
 
+from . import tune as _tune
+
+_tune.load_table()
+
 __all__ = [
-    "AzebanError", "supported_lengths", "FFT", "FFT_BACKWARD", "FFT_FORWARD", "Grid",
+    "AzebanError", "supported_lengths", "FFT", "FFT_BACKWARD", "FFT_FORWARD", "Grid", "Group",
     "IncompressibleEuler", "NoViscosity", "Quadratic", "Simulation", "SmoothCutoff1D", "SSP_RK3",
     "Step1D", "leray", "make_fft", "make_grid", "make_viscosity", "next_good_size",
     "precision_code",

@@ -31,6 +31,9 @@ EXPORTS = [
     "az_sim_state",
     "az_fft_create", "az_fft_destroy", "az_fft_forward", "az_fft_backward", "az_fft_work_area_size",
     "az_leray", "az_profile_enable", "az_profile_read", "az_euler_dudt_noalloc",
+    "az_tune_set", "az_tune_get", "az_euler_diagnostics",
+    "az_sim_member_start", "az_sim_member_stop", "az_group_create", "az_group_destroy",
+    "az_group_steps", "az_group_set_end", "az_group_simulate_until",
 ]
 
 
@@ -92,6 +95,16 @@ def _load():
         "az_profile_enable": (I, [I]),
         "az_profile_read": (I, [ct.POINTER(D), ct.POINTER(D), ct.POINTER(LL), I]),
         "az_euler_dudt_noalloc": (I, [I, LL, LL, I, ct.POINTER(az_visc), P, P, P]),
+        "az_tune_set": (I, [I, I, I, I]),
+        "az_tune_get": (I, [I, I, I, ct.POINTER(I)]),
+        "az_euler_diagnostics": (I, [P, P, P, ct.POINTER(D), ct.POINTER(D)]),
+        "az_sim_member_start": (I, [P, I, P, D, P]),
+        "az_sim_member_stop": (I, [P, I, P]),
+        "az_group_create": (I, [ct.POINTER(P), I, ct.POINTER(P)]),
+        "az_group_destroy": (I, [P]),
+        "az_group_steps": (I, [P, I, P]),
+        "az_group_set_end": (I, [P, D, P]),
+        "az_group_simulate_until": (I, [P, D, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

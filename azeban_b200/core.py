@@ -269,6 +269,14 @@ class IncompressibleEuler:
         check(lib.az_euler_dudt(self._h, dudt_hat.data_ptr(), u_hat.data_ptr(), float(t), float(dt),
                                 float(C), _stream_ptr(stream)))
 
+    def diagnostics(self, u_hat, stream=None):
+        """Kinetic energy and enstrophy per member (FP64, compensated sums)."""
+        self._check(u_hat, "u_hat")
+        e = (ct.c_double * self.batch)()
+        w = (ct.c_double * self.batch)()
+        check(lib.az_euler_diagnostics(self._h, u_hat.data_ptr(), _stream_ptr(stream), e, w))
+        return (e[0], w[0]) if self.batch == 1 else (list(e), list(w))
+
     def dt(self, C: float, stream=None):
         """Equation::dt (incompressible_euler.hpp:122-124), per member."""
         out = (ct.c_double * self.batch)()
@@ -337,6 +345,18 @@ class Simulation:
     def steps(self, n: int, stream=None):
         check(lib.az_sim_steps(self._h, int(n), _stream_ptr(stream)))
 
+    def member_start(self, member: int, u_hat_member, t_end: float, stream=None):
+        """Copies one member's state into slot `member` and restarts its clock
+        at 0 with end t_end (continuous batching)."""
+        base = self.grid.shape_fourier(self.grid.dim)
+        _check_tensor(u_hat_member, "u_hat_member", self._dtype, base)
+        check(lib.az_sim_member_start(self._h, int(member), u_hat_member.data_ptr(), float(t_end),
+                                      _stream_ptr(stream)))
+
+    def member_stop(self, member: int, stream=None):
+        """Frees slot `member`: it is skipped until started again."""
+        check(lib.az_sim_member_stop(self._h, int(member), _stream_ptr(stream)))
+
     def u(self):
         """A torch view of the device state (valid while the Simulation lives)."""
         ptr = lib.az_sim_u(self._h)
@@ -355,6 +375,33 @@ class Simulation:
 
     def time_all(self, stream=None):
         return self.state(stream)[0]
+
+
+class Group:
+    """Several simulations (any dimension, size, precision) advanced together,
+    one captured graph per SSP-RK3 step with one branch per simulation."""
+
+    def __init__(self, sims):
+        self.sims = list(sims)
+        arr = (ct.c_void_p * len(self.sims))(*[s._h for s in self.sims])
+        h = ct.c_void_p()
+        check(lib.az_group_create(arr, len(self.sims), ct.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib.az_group_destroy(h)
+            self._h = None
+
+    def steps(self, n: int, stream=None):
+        check(lib.az_group_steps(self._h, int(n), _stream_ptr(stream)))
+
+    def set_end(self, t: float, stream=None):
+        check(lib.az_group_set_end(self._h, float(t), _stream_ptr(stream)))
+
+    def simulate_until(self, t: float, stream=None):
+        check(lib.az_group_simulate_until(self._h, float(t), _stream_ptr(stream)))
 
 
 def _tensor_from_ptr(ptr, shape, dtype):

@@ -62,9 +62,10 @@ struct ColArgs {
 
 // Batched column transforms along a strided axis.  grid = (ntile * nouter,
 // ncomp, nmembers); block = NC * L/E threads.
-template <typename T, int L, int NC, int S, int MODE>
-__global__ void __launch_bounds__(NC * Plan<L>::TPL) k_cols(ColArgs a) {
+template <typename T, int L, int NC, int S, int MODE, int V>
+__global__ void __launch_bounds__(NC * Plan<L, V>::TPL) k_cols(ColArgs a) {
   using C = cvec<T>;
+  using P = Plan<L, V>;
   extern __shared__ __align__(16) unsigned char az_smem[];
   C* tw = reinterpret_cast<C*>(az_smem);
   C* sm = tw + L;
@@ -103,7 +104,7 @@ __global__ void __launch_bounds__(NC * Plan<L>::TPL) k_cols(ColArgs a) {
     if constexpr (MODE == COL_TRUNC) dst = retained_row(m, n, L);
     if (valid && dst >= 0) out[dst * a.out_row] = v;
   };
-  fft_columns<C, S, L, NC, false>(sm, tw, col, tl, load, store);
+  fft_columns<C, S, L, NC, false, P>(sm, tw, col, tl, load, store);
 }
 
 struct RowArgs {
@@ -144,19 +145,21 @@ __device__ __forceinline__ C herm_bin(const C* line, int nh, int m, int stride =
 
 // Contiguous-axis pass of the right-hand side: for each pair of lines, the
 // inverse real transform of the DIM velocity components (two real signals per
-// complex transform), the CFL maximum, the products B = u (x) u in the
+// complex transform, the first stage loaded straight from global memory with
+// the Hermitian extension), the CFL maximum, the products B = u (x) u in the
 // reference's component order, and the forward real transform of the
 // products, of which only bins [0, nh) are written.
 // grid = (ceil(nlines / (2 NLP)), nmembers); block = NB * NLP * L/E.
-template <typename T, int L, int NLP, int DIM>
-__global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NLP * Plan<L>::TPL)
+template <typename T, int L, int NLP, int DIM, int V>
+__global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NLP * Plan<L, V>::TPL)
     k_rows_product(RowArgs a) {
   using C = cvec<T>;
+  using P = Plan<L, V>;
   constexpr int NB = DIM * (DIM + 1) / 2;
   constexpr int NINV = DIM * NLP;
   constexpr int NFWD = NB * NLP;
   constexpr int SROW = NFWD + 1;
-  constexpr int TPL = Plan<L>::TPL;
+  constexpr int TPL = P::TPL;
   constexpr int NT = NFWD * TPL;
   extern __shared__ __align__(16) unsigned char az_smem[];
   C* tw = reinterpret_cast<C*>(az_smem);
@@ -169,40 +172,34 @@ __global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NLP * Plan<L>::TPL)
   const C* in = reinterpret_cast<const C*>(a.in) + member * a.in_mem;
   C* out = reinterpret_cast<C*>(a.out) + member * a.out_mem;
   load_twiddles<C, L>(tw, reinterpret_cast<const C*>(a.tw));
-
-  // 1. Load and pack: column (p, q) holds signal 2q + i * signal 2q+1 of the
-  //    line pair p, signal s = component s % DIM of line (s / DIM).
-  for (int idx = tid; idx < NINV * L; idx += NT) {
-    const int m = idx % L;
-    const int cz = idx / L;
-    const int p = cz / DIM;
-    const int q = cz % DIM;
-    C x[2];
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int s = 2 * q + h;
-      const long long ln = line0 + 2 * p + s / DIM;
-      const C* src = ln < a.nlines ? in + ln * a.in_line + (s % DIM) : nullptr;
-      x[h] = herm_bin<C, L>(src, a.nh, m, DIM);
-    }
-    sm[m * SROW + cz] = cmk<C>(x[0].x - x[1].y, x[0].y + x[1].x);
-  }
   __syncthreads();
 
-  // 2. Inverse transforms of the NINV packed columns.
+  // 1. Inverse transforms.  Column col = (pair p, slot q) holds signal 2q +
+  //    i * signal 2q+1, signal s = component s % DIM of line s / DIM of the
+  //    pair; its first stage reads global memory directly.
   {
     const bool active = tid < NINV * TPL;
     const int col = active ? tid % NINV : 0;
     const int tl = active ? tid / NINV : 0;
-    fft_columns<C, +1, L, SROW, true>(
-        sm, tw, col, tl, [&](int m) { return sm[m * SROW + col]; },
-        [&](int m, C v) {
-          if (active) sm[m * SROW + col] = v;
-        });
+    const int p = col / DIM;
+    const int q = col % DIM;
+    const long long l0 = line0 + 2 * p + (2 * q) / DIM;
+    const long long l1 = line0 + 2 * p + (2 * q + 1) / DIM;
+    const C* src0 = (active && l0 < a.nlines) ? in + l0 * a.in_line + (2 * q) % DIM : nullptr;
+    const C* src1 = (active && l1 < a.nlines) ? in + l1 * a.in_line + (2 * q + 1) % DIM : nullptr;
+    const int nh = a.nh;
+    fft_columns<C, +1, L, SROW, true, P>(
+        sm, tw, col, tl,
+        [&](int m) {
+          const C x = herm_bin<C, L>(src0, nh, m, DIM);
+          const C y = herm_bin<C, L>(src1, nh, m, DIM);
+          return cmk<C>(x.x - y.y, x.y + y.x);
+        },
+        [&](int m, C v) { sm[m * SROW + col] = v; }, active);
   }
   __syncthreads();
 
-  // 3. CFL maximum and products.
+  // 2. CFL maximum and products.
   constexpr int MAXI = (NLP * L + NT - 1) / NT;
   T sv[MAXI][2 * DIM];
   T vmax = T(0);
@@ -255,33 +252,36 @@ __global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NLP * Plan<L>::TPL)
   }
   __syncthreads();
 
-  // 4. Forward transforms of the NFWD product columns (product c of line a
+  // 3. Forward transforms of the NFWD product columns (product c of line a
   //    in the real part, of line b in the imaginary part).
   {
     const int col = tid % NFWD;
     const int tl = tid / NFWD;
-    fft_columns<C, -1, L, SROW, true>(
+    fft_columns<C, -1, L, SROW, true, P>(
         sm, tw, col, tl, [&](int m) { return sm[m * SROW + col]; },
         [&](int m, C v) { sm[m * SROW + col] = v; });
   }
   __syncthreads();
 
-  // 5. Separate the two real spectra and write bins [0, nh), component
+  // 4. Separate the two real spectra and write bins [0, nh), component
   //    fastest so the stores of a line are contiguous.
-  const int per_pair = NB * a.nh;
-  for (int idx = tid; idx < NLP * per_pair; idx += NT) {
-    const int p = idx / per_pair;
-    const int r = idx - p * per_pair;
-    const int k = r / NB;
-    const int c = r - k * NB;
-    const int cf = p * NB + c;
-    const C fk = sm[k * SROW + cf];
-    const C fm = sm[((L - k) % L) * SROW + cf];
-    const C xa = cmk<C>(T(0.5) * (fk.x + fm.x), T(0.5) * (fk.y - fm.y));
-    const C xb = cmk<C>(T(0.5) * (fk.y + fm.y), T(-0.5) * (fk.x - fm.x));
+  const int nb_nh = NB * a.nh;
+#pragma unroll 1
+  for (int p = 0; p < NLP; ++p) {
     const long long la = line0 + 2 * p;
-    if (la < a.nlines) out[la * a.out_line + r] = xa;
-    if (la + 1 < a.nlines) out[(la + 1) * a.out_line + r] = xb;
+    C* oa = out + la * a.out_line;
+    C* ob = oa + a.out_line;
+    const bool va = la < a.nlines;
+    const bool vb = la + 1 < a.nlines;
+    for (int r = tid; r < nb_nh; r += NT) {
+      const int k = r / NB;
+      const int c = r - k * NB;
+      const int cf = p * NB + c;
+      const C fk = sm[k * SROW + cf];
+      const C fm = sm[(k == 0 ? 0 : L - k) * SROW + cf];
+      if (va) oa[r] = cmk<C>(T(0.5) * (fk.x + fm.x), T(0.5) * (fk.y - fm.y));
+      if (vb) ob[r] = cmk<C>(T(0.5) * (fk.y + fm.y), T(-0.5) * (fk.x - fm.x));
+    }
   }
 
   // CFL reduction: warp, then block, then one atomic per CTA.
@@ -360,14 +360,15 @@ template <typename T> __device__ __forceinline__ T visc_eval(const Visc& v, T k)
 //   MODE_RK2:  out = 3/4 u0 + 1/4 (u + dt dudt)       (ssp_rk3.hpp:57-58)
 //   MODE_RK3:  out = 2/3 (u + dt dudt) + 1/3 u0       (ssp_rk3.hpp:60-61)
 // grid = (ntile, nmembers); block = NB * NCM * L/E.
-template <typename T, int L, int NCM, int DIM>
-__global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NCM * Plan<L>::TPL)
+template <typename T, int L, int NCM, int DIM, int V>
+__global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NCM * Plan<L, V>::TPL)
     k_fwd_epilogue(EpiArgs a) {
   using C = cvec<T>;
+  using P = Plan<L, V>;
   constexpr int NB = DIM * (DIM + 1) / 2;
   constexpr int NC = NB * NCM;
   constexpr int SROW = NC;
-  constexpr int TPL = Plan<L>::TPL;
+  constexpr int TPL = P::TPL;
   constexpr int NT = NC * TPL;
   extern __shared__ __align__(16) unsigned char az_smem[];
   C* tw = reinterpret_cast<C*>(az_smem);
@@ -387,7 +388,7 @@ __global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NCM * Plan<L>::TPL)
     const long long p = (long long)tile * NCM + pl;
     const bool valid = p < a.ninner;
     const C* Bp = reinterpret_cast<const C*>(a.B) + member * a.B_mem + (long long)tile * NC + col;
-    fft_columns<C, -1, L, SROW, true>(
+    fft_columns<C, -1, L, SROW, true, P>(
         sm, tw, col, tl,
         [&](int m) -> C { return valid ? Bp[m * a.B_row] : cmk<C>(T(0), T(0)); },
         [&](int m, C v) {
@@ -496,11 +497,12 @@ struct RealRowArgs {
 };
 
 // c2r: lines of L/2+1 complex -> L real.  grid = ceil(nlines / (2 NLP)).
-template <typename T, int L, int NLP>
-__global__ void __launch_bounds__(NLP * Plan<L>::TPL) k_rows_c2r(RealRowArgs a) {
+template <typename T, int L, int NLP, int V>
+__global__ void __launch_bounds__(NLP * Plan<L, V>::TPL) k_rows_c2r(RealRowArgs a) {
   using C = cvec<T>;
+  using P = Plan<L, V>;
   constexpr int SROW = NLP + 1;
-  constexpr int NT = NLP * Plan<L>::TPL;
+  constexpr int NT = NLP * P::TPL;
   constexpr int LH = L / 2 + 1;
   extern __shared__ __align__(16) unsigned char az_smem[];
   C* tw = reinterpret_cast<C*>(az_smem);
@@ -522,7 +524,7 @@ __global__ void __launch_bounds__(NLP * Plan<L>::TPL) k_rows_c2r(RealRowArgs a) 
   {
     const int col = tid % NLP;
     const int tl = tid / NLP;
-    fft_columns<C, +1, L, SROW, true>(
+    fft_columns<C, +1, L, SROW, true, P>(
         sm, tw, col, tl, [&](int m) { return sm[m * SROW + col]; },
         [&](int m, C v) { sm[m * SROW + col] = v; });
   }
@@ -539,11 +541,12 @@ __global__ void __launch_bounds__(NLP * Plan<L>::TPL) k_rows_c2r(RealRowArgs a) 
 }
 
 // r2c: lines of L real -> L/2+1 complex.  grid = ceil(nlines / (2 NLP)).
-template <typename T, int L, int NLP>
-__global__ void __launch_bounds__(NLP * Plan<L>::TPL) k_rows_r2c(RealRowArgs a) {
+template <typename T, int L, int NLP, int V>
+__global__ void __launch_bounds__(NLP * Plan<L, V>::TPL) k_rows_r2c(RealRowArgs a) {
   using C = cvec<T>;
+  using P = Plan<L, V>;
   constexpr int SROW = NLP + 1;
-  constexpr int NT = NLP * Plan<L>::TPL;
+  constexpr int NT = NLP * P::TPL;
   constexpr int LH = L / 2 + 1;
   extern __shared__ __align__(16) unsigned char az_smem[];
   C* tw = reinterpret_cast<C*>(az_smem);
@@ -565,7 +568,7 @@ __global__ void __launch_bounds__(NLP * Plan<L>::TPL) k_rows_r2c(RealRowArgs a) 
   {
     const int col = tid % NLP;
     const int tl = tid / NLP;
-    fft_columns<C, -1, L, SROW, true>(
+    fft_columns<C, -1, L, SROW, true, P>(
         sm, tw, col, tl, [&](int m) { return sm[m * SROW + col]; },
         [&](int m, C v) { sm[m * SROW + col] = v; });
   }

@@ -50,32 +50,44 @@ template <int S, typename C> __device__ __forceinline__ C cmul_si(C a) {
   else return cmk<C>(a.y, -a.x);
 }
 
-// cos(2 pi m / 48) for m in [0, 12], the quarter table every radix up to 16
-// (and 6, 12) needs.  Closed forms evaluated to 25 digits.
-__host__ __device__ constexpr double cos48_q(int m) {
-  constexpr double q[13] = {1.0,
+// cos(2 pi m / 96) for m in [0, 24], the quarter table every radix in
+// {2,3,4,6,8,12,16,24,32,48} needs.  Closed forms evaluated to 25 digits.
+__host__ __device__ constexpr double cos96_q(int m) {
+  constexpr double q[25] = {1.0,
+                            0.9978589232386035067380698,
                             0.9914448613738104111445575,
+                            0.9807852804032304491261822,
                             0.9659258262890682867497432,
+                            0.9469301294951056642558043,
                             0.9238795325112867561281832,
+                            0.8968727415326883038941039,
                             0.8660254037844386467637232,
+                            0.8314696123025452370787884,
                             0.7933533402912351645797770,
+                            0.7518398074789773964075194,
                             0.7071067811865475244008444,
+                            0.6593458151000688684251246,
                             0.6087614290087206394160975,
+                            0.5555702330196022247428308,
                             0.5,
+                            0.4422886902190012819952390,
                             0.3826834323650897717284600,
+                            0.3214394653031615807010576,
                             0.2588190451025207623488988,
+                            0.1950903220161282678482849,
                             0.1305261922200515915484062,
+                            0.0654031292301430668153156,
                             0.0};
   return q[m];
 }
-__host__ __device__ constexpr double cos48(int m) {
-  m = ((m % 48) + 48) % 48;
-  if (m <= 12) return cos48_q(m);
-  if (m <= 24) return -cos48_q(24 - m);
-  if (m <= 36) return -cos48_q(m - 24);
-  return cos48_q(48 - m);
+__host__ __device__ constexpr double cos96(int m) {
+  m = ((m % 96) + 96) % 96;
+  if (m <= 24) return cos96_q(m);
+  if (m <= 48) return -cos96_q(48 - m);
+  if (m <= 72) return -cos96_q(m - 48);
+  return cos96_q(96 - m);
 }
-__host__ __device__ constexpr double sin48(int m) { return cos48(m - 12); }
+__host__ __device__ constexpr double sin96(int m) { return cos96(m - 24); }
 
 // z * w_R^{S*m}, w_R = exp(2 pi i / R), with exact special cases.
 template <int R, int S, int M, typename C> __device__ __forceinline__ C rot(C z) {
@@ -90,9 +102,10 @@ template <int R, int S, int M, typename C> __device__ __forceinline__ C rot(C z)
     return cmul_si<-S>(z);
   } else {
     using T = decltype(C::x);
-    constexpr int m48 = m * (48 / R);
-    const T c = T(cos48(m48));
-    const T s = T(S * sin48(m48));
+    static_assert(96 % R == 0, "radix must divide 96");
+    constexpr int m96 = m * (96 / R);
+    const T c = T(cos96(m96));
+    const T s = T(S * sin96(m96));
     return cmk<C>(z.x * c - z.y * s, z.x * s + z.y * c);
   }
 }
@@ -105,6 +118,9 @@ template <> struct Split<6> { static constexpr int R1 = 2, R2 = 3; };
 template <> struct Split<8> { static constexpr int R1 = 2, R2 = 4; };
 template <> struct Split<12> { static constexpr int R1 = 4, R2 = 3; };
 template <> struct Split<16> { static constexpr int R1 = 4, R2 = 4; };
+template <> struct Split<24> { static constexpr int R1 = 8, R2 = 3; };
+template <> struct Split<32> { static constexpr int R1 = 4, R2 = 8; };
+template <> struct Split<48> { static constexpr int R1 = 16, R2 = 3; };
 
 template <int R, int S, typename C> struct DFT;
 
@@ -190,32 +206,52 @@ template <int R, int S, typename C> struct DFT {
 // ---------------------------------------------------------------------------
 template <int... Rs> struct Radices {};
 
-template <int L> struct Plan;
-#define AZB_PLAN(Lv, Ev, ...)                           \
-  template <> struct Plan<Lv> {                          \
+// Variant 0 ("std") keeps E <= 24; variant 1 ("wide") trades registers for
+// fewer stages (one shared-memory exchange per transform where E <= 48 allows).
+template <int L, int V = 0> struct Plan;
+#define AZB_PLAN(Lv, Vv, Ev, ...)                        \
+  template <> struct Plan<Lv, Vv> {                      \
     static constexpr int L = Lv;                         \
     static constexpr int E = Ev;                         \
     static constexpr int TPL = Lv / Ev;                  \
     using R = Radices<__VA_ARGS__>;                      \
   };
-AZB_PLAN(4, 4, 4)
-AZB_PLAN(6, 6, 6)
-AZB_PLAN(8, 8, 8)
-AZB_PLAN(12, 12, 12)
-AZB_PLAN(16, 16, 16)
-AZB_PLAN(24, 24, 8, 3)
-AZB_PLAN(32, 8, 8, 4)
-AZB_PLAN(48, 24, 8, 6)
-AZB_PLAN(64, 8, 8, 8)
-AZB_PLAN(96, 24, 8, 12)
-AZB_PLAN(128, 16, 8, 16)
-AZB_PLAN(192, 24, 8, 4, 6)
-AZB_PLAN(256, 16, 16, 16)
-AZB_PLAN(384, 24, 8, 8, 6)
-AZB_PLAN(512, 8, 8, 8, 8)
-AZB_PLAN(768, 24, 8, 8, 12)
-AZB_PLAN(1024, 16, 16, 4, 16)
-AZB_PLAN(1536, 24, 8, 8, 8, 3)
+AZB_PLAN(4, 0, 4, 4)
+AZB_PLAN(6, 0, 6, 6)
+AZB_PLAN(8, 0, 8, 8)
+AZB_PLAN(12, 0, 12, 12)
+AZB_PLAN(16, 0, 16, 16)
+AZB_PLAN(24, 0, 24, 8, 3)
+AZB_PLAN(32, 0, 8, 8, 4)
+AZB_PLAN(48, 0, 24, 8, 6)
+AZB_PLAN(64, 0, 8, 8, 8)
+AZB_PLAN(96, 0, 24, 8, 12)
+AZB_PLAN(128, 0, 16, 8, 16)
+AZB_PLAN(192, 0, 24, 8, 4, 6)
+AZB_PLAN(256, 0, 16, 16, 16)
+AZB_PLAN(384, 0, 24, 8, 8, 6)
+AZB_PLAN(512, 0, 8, 8, 8, 8)
+AZB_PLAN(768, 0, 24, 8, 8, 12)
+AZB_PLAN(1024, 0, 16, 16, 4, 16)
+AZB_PLAN(1536, 0, 24, 8, 8, 8, 3)
+AZB_PLAN(4, 1, 4, 4)
+AZB_PLAN(6, 1, 6, 6)
+AZB_PLAN(8, 1, 8, 8)
+AZB_PLAN(12, 1, 12, 12)
+AZB_PLAN(16, 1, 16, 16)
+AZB_PLAN(24, 1, 24, 24)
+AZB_PLAN(32, 1, 32, 32)
+AZB_PLAN(48, 1, 48, 48)
+AZB_PLAN(64, 1, 16, 16, 4)
+AZB_PLAN(96, 1, 24, 8, 12)
+AZB_PLAN(128, 1, 16, 8, 16)
+AZB_PLAN(192, 1, 24, 8, 24)
+AZB_PLAN(256, 1, 16, 16, 16)
+AZB_PLAN(384, 1, 48, 16, 24)
+AZB_PLAN(512, 1, 32, 16, 32)
+AZB_PLAN(768, 1, 48, 16, 48)
+AZB_PLAN(1024, 1, 32, 32, 32)
+AZB_PLAN(1536, 1, 48, 16, 4, 24)
 #undef AZB_PLAN
 
 template <typename RL> struct RadixInfo;
@@ -318,10 +354,10 @@ struct Engine {
 //   store(row, C)      receives output bin `row`
 // SYNC_STORE: put a barrier before the stores (needed when they go to sm).
 // Threads with active == false take part in the barriers only.
-template <typename C, int S, int L, int SROW, bool SYNC_STORE, typename Load, typename Store>
+template <typename C, int S, int L, int SROW, bool SYNC_STORE, typename P = Plan<L>, typename Load,
+          typename Store>
 __device__ __forceinline__ void fft_columns(C* sm, const C* tw, int col, int tl, Load&& load,
                                             Store&& store, bool active = true) {
-  using P = Plan<L>;
   using Info = RadixInfo<typename P::R>;
   using Eng = Engine<C, S, L, P::E, SROW>;
   C v[P::E];

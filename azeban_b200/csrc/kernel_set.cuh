@@ -22,15 +22,16 @@ struct TileShape {
   int nlpr;   // line pairs per CTA, plain r2c / c2r
 };
 
+// Every launcher takes the plan variant v (0 std, 1 wide; see Plan<L, V>).
 struct KernelSet {
   int L;
   int precision;  // 0 FP64, 1 FP32
-  TileShape tiles;
-  cudaError_t (*cols)(int kind, const ColArgs&, unsigned gx, unsigned gy, unsigned gz, cudaStream_t);
-  cudaError_t (*rows_product)(int dim, const RowArgs&, unsigned gx, unsigned gy, cudaStream_t);
-  cudaError_t (*epilogue)(int dim, const EpiArgs&, unsigned gx, unsigned gy, cudaStream_t);
-  cudaError_t (*c2r)(const RealRowArgs&, unsigned gx, cudaStream_t);
-  cudaError_t (*r2c)(const RealRowArgs&, unsigned gx, cudaStream_t);
+  TileShape tiles[2];  // per plan variant
+  cudaError_t (*cols)(int v, int kind, const ColArgs&, unsigned gx, unsigned gy, unsigned gz, cudaStream_t);
+  cudaError_t (*rows_product)(int v, int dim, const RowArgs&, unsigned gx, unsigned gy, cudaStream_t);
+  cudaError_t (*epilogue)(int v, int dim, const EpiArgs&, unsigned gx, unsigned gy, cudaStream_t);
+  cudaError_t (*c2r)(int v, const RealRowArgs&, unsigned gx, cudaStream_t);
+  cudaError_t (*r2c)(int v, const RealRowArgs&, unsigned gx, cudaStream_t);
 };
 
 constexpr int kpow2floor(int x) {
@@ -40,7 +41,7 @@ constexpr int kpow2floor(int x) {
 }
 constexpr int kclamp(int x, int lo, int hi) { return x < lo ? lo : (x > hi ? hi : x); }
 
-template <typename T, int L> struct Tiles {
+template <typename T, int L, int V> struct Tiles {
   static constexpr int CB = int(sizeof(cvec<T>));
   static constexpr int NC = kclamp(kpow2floor(49152 / (L * CB)), 2, 32);
   static constexpr int NLP3 = kclamp(kpow2floor(81920 / (L * 6 * CB)), 1, 16);
@@ -55,25 +56,23 @@ template <typename K> inline cudaError_t set_smem(K kernel, size_t bytes) {
   return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
 }
 
-template <typename T, int L> struct Launch {
+template <typename T, int L, int V> struct LaunchV {
   using C = cvec<T>;
-  using TS = Tiles<T, L>;
-  static constexpr int TPL = Plan<L>::TPL;
+  using TS = Tiles<T, L, V>;
+  static constexpr int TPL = Plan<L, V>::TPL;
 
   template <int S, int MODE>
   static cudaError_t col_kernel(const ColArgs& a, dim3 g, cudaStream_t st) {
     constexpr int NC = TS::NC;
     const size_t smem = size_t(L + L * NC) * sizeof(C);
-    auto k = k_cols<T, L, NC, S, MODE>;
+    auto k = k_cols<T, L, NC, S, MODE, V>;
     static const cudaError_t attr = set_smem(k, smem);
     if (attr != cudaSuccess) return attr;
     k<<<g, NC * TPL, smem, st>>>(a);
     return cudaGetLastError();
   }
 
-  static cudaError_t cols(int kind, const ColArgs& a, unsigned gx, unsigned gy, unsigned gz,
-                          cudaStream_t st) {
-    const dim3 g(gx, gy, gz);
+  static cudaError_t cols(int kind, const ColArgs& a, dim3 g, cudaStream_t st) {
     switch (kind) {
       case COLK_PAD_INV: return col_kernel<+1, COL_PAD>(a, g, st);
       case COLK_PLAIN_INV: return col_kernel<+1, COL_PLAIN>(a, g, st);
@@ -87,16 +86,14 @@ template <typename T, int L> struct Launch {
   static cudaError_t rows_kernel(const RowArgs& a, dim3 g, cudaStream_t st) {
     constexpr int NB = DIM * (DIM + 1) / 2;
     const size_t smem = size_t(L + L * (NB * NLP + 1)) * sizeof(C);
-    auto k = k_rows_product<T, L, NLP, DIM>;
+    auto k = k_rows_product<T, L, NLP, DIM, V>;
     static const cudaError_t attr = set_smem(k, smem);
     if (attr != cudaSuccess) return attr;
     k<<<g, NB * NLP * TPL, smem, st>>>(a);
     return cudaGetLastError();
   }
 
-  static cudaError_t rows_product(int dim, const RowArgs& a, unsigned gx, unsigned gy,
-                                  cudaStream_t st) {
-    const dim3 g(gx, gy, 1);
+  static cudaError_t rows(int dim, const RowArgs& a, dim3 g, cudaStream_t st) {
     if (dim == 2) return rows_kernel<2, TS::NLP2>(a, g, st);
     if (dim == 3) return rows_kernel<3, TS::NLP3>(a, g, st);
     return cudaErrorInvalidValue;
@@ -106,16 +103,14 @@ template <typename T, int L> struct Launch {
   static cudaError_t epi_kernel(const EpiArgs& a, dim3 g, cudaStream_t st) {
     constexpr int NB = DIM * (DIM + 1) / 2;
     const size_t smem = size_t(L + L * NB * NCM) * sizeof(C);
-    auto k = k_fwd_epilogue<T, L, NCM, DIM>;
+    auto k = k_fwd_epilogue<T, L, NCM, DIM, V>;
     static const cudaError_t attr = set_smem(k, smem);
     if (attr != cudaSuccess) return attr;
     k<<<g, NB * NCM * TPL, smem, st>>>(a);
     return cudaGetLastError();
   }
 
-  static cudaError_t epilogue(int dim, const EpiArgs& a, unsigned gx, unsigned gy,
-                              cudaStream_t st) {
-    const dim3 g(gx, gy, 1);
+  static cudaError_t epi(int dim, const EpiArgs& a, dim3 g, cudaStream_t st) {
     if (dim == 2) return epi_kernel<2, TS::NCM2>(a, g, st);
     if (dim == 3) return epi_kernel<3, TS::NCM3>(a, g, st);
     return cudaErrorInvalidValue;
@@ -124,7 +119,7 @@ template <typename T, int L> struct Launch {
   static cudaError_t c2r(const RealRowArgs& a, unsigned gx, cudaStream_t st) {
     constexpr int NLP = TS::NLPR;
     const size_t smem = size_t(L + L * (NLP + 1)) * sizeof(C);
-    auto k = k_rows_c2r<T, L, NLP>;
+    auto k = k_rows_c2r<T, L, NLP, V>;
     static const cudaError_t attr = set_smem(k, smem);
     if (attr != cudaSuccess) return attr;
     k<<<gx, NLP * TPL, smem, st>>>(a);
@@ -134,23 +129,47 @@ template <typename T, int L> struct Launch {
   static cudaError_t r2c(const RealRowArgs& a, unsigned gx, cudaStream_t st) {
     constexpr int NLP = TS::NLPR;
     const size_t smem = size_t(L + L * (NLP + 1)) * sizeof(C);
-    auto k = k_rows_r2c<T, L, NLP>;
+    auto k = k_rows_r2c<T, L, NLP, V>;
     static const cudaError_t attr = set_smem(k, smem);
     if (attr != cudaSuccess) return attr;
     k<<<gx, NLP * TPL, smem, st>>>(a);
     return cudaGetLastError();
   }
 
+  static TileShape tiles() { return {TS::NC, TS::NLP2, TS::NLP3, TS::NCM2, TS::NCM3, TS::NLPR}; }
+};
+
+template <typename T, int L> struct Launch {
+  static cudaError_t cols(int v, int kind, const ColArgs& a, unsigned gx, unsigned gy, unsigned gz,
+                          cudaStream_t st) {
+    const dim3 g(gx, gy, gz);
+    return v ? LaunchV<T, L, 1>::cols(kind, a, g, st) : LaunchV<T, L, 0>::cols(kind, a, g, st);
+  }
+  static cudaError_t rows_product(int v, int dim, const RowArgs& a, unsigned gx, unsigned gy,
+                                  cudaStream_t st) {
+    const dim3 g(gx, gy, 1);
+    return v ? LaunchV<T, L, 1>::rows(dim, a, g, st) : LaunchV<T, L, 0>::rows(dim, a, g, st);
+  }
+  static cudaError_t epilogue(int v, int dim, const EpiArgs& a, unsigned gx, unsigned gy,
+                              cudaStream_t st) {
+    const dim3 g(gx, gy, 1);
+    return v ? LaunchV<T, L, 1>::epi(dim, a, g, st) : LaunchV<T, L, 0>::epi(dim, a, g, st);
+  }
+  static cudaError_t c2r(int v, const RealRowArgs& a, unsigned gx, cudaStream_t st) {
+    return v ? LaunchV<T, L, 1>::c2r(a, gx, st) : LaunchV<T, L, 0>::c2r(a, gx, st);
+  }
+  static cudaError_t r2c(int v, const RealRowArgs& a, unsigned gx, cudaStream_t st) {
+    return v ? LaunchV<T, L, 1>::r2c(a, gx, st) : LaunchV<T, L, 0>::r2c(a, gx, st);
+  }
   static const KernelSet* get() {
-    static const KernelSet ks = {
-        L,
-        sizeof(T) == 8 ? 0 : 1,
-        {TS::NC, TS::NLP2, TS::NLP3, TS::NCM2, TS::NCM3, TS::NLPR},
-        &cols,
-        &rows_product,
-        &epilogue,
-        &c2r,
-        &r2c};
+    static const KernelSet ks = {L,
+                                 sizeof(T) == 8 ? 0 : 1,
+                                 {LaunchV<T, L, 0>::tiles(), LaunchV<T, L, 1>::tiles()},
+                                 &cols,
+                                 &rows_product,
+                                 &epilogue,
+                                 &c2r,
+                                 &r2c};
     return &ks;
   }
 };

@@ -94,6 +94,10 @@ az_status az_euler_dudt_noalloc(int dim, long long N_phys, long long N_phys_pad,
   e.ks = ks;
   e.csize = precision == AZ_PREC_F64 ? 16 : 8;
   e.prof = false;
+  const int kbase = dim == 2 ? 3 : 0;
+  e.v_cols = tuned_variant(precision, int(N_phys_pad), kbase + 0);
+  e.v_rows = tuned_variant(precision, int(N_phys_pad), kbase + 1);
+  e.v_epi = tuned_variant(precision, int(N_phys_pad), kbase + 2);
   const long long N = e.N, M = e.M, Nh = e.Nh;
   if (dim == 3) {
     e.buf_mem[0] = 6 * M * N * Nh;

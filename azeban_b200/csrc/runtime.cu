@@ -5,6 +5,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -42,6 +43,26 @@ static const int kLengths[] = {
     AZB_LENGTHS(AZB_LIST)
 #undef AZB_LIST
 };
+
+// ---------------------------------------------------------------------------
+// Tuning table: plan variant per (precision, length, pass kind).  Defaults:
+// FP32 uses the wide plans (fewer exchanges), FP64 the register-lean ones.
+// AZ_PLAN_VARIANT="c,r,e" overrides every entry; az_tune_set overrides one.
+// ---------------------------------------------------------------------------
+static std::mutex g_tune_mutex;
+static std::map<std::tuple<int, int, int>, int> g_tune;
+
+int tuned_variant(int precision, int L, int kind) {
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  auto it = g_tune.find(std::make_tuple(precision, L, kind));
+  if (it != g_tune.end()) return it->second;
+  if (const char* env = std::getenv("AZ_PLAN_VARIANT")) {
+    int v[3] = {0, 0, 0};
+    if (std::sscanf(env, "%d,%d,%d", &v[0], &v[1], &v[2]) == 3 && kind >= 0 && kind < 6)
+      return v[kind % 3] ? 1 : 0;
+  }
+  return precision == 1 ? 1 : 0;
+}
 
 // ---------------------------------------------------------------------------
 // Errors
@@ -199,6 +220,10 @@ az_status az_euler_create(const az_euler_desc* d, az_euler* out) {
   e->eps_visc = d->visc.type == AZ_VISC_NONE ? 0.0 : d->visc.eps;
   e->ks = ks;
   e->csize = d->precision == 0 ? 16 : 8;
+  const int kbase = e->dim == 2 ? 3 : 0;
+  e->v_cols = tuned_variant(e->prec, int(e->M), kbase + 0);
+  e->v_rows = tuned_variant(e->prec, int(e->M), kbase + 1);
+  e->v_epi = tuned_variant(e->prec, int(e->M), kbase + 2);
   const long long N = e->N, M = e->M, Nh = e->Nh;
   if (e->dim == 3) {
     e->buf_mem[0] = 6 * M * N * Nh;  // A1 [M][N][Nh][3], later B2 [M][N][Nh][6]
@@ -244,6 +269,14 @@ az_status az_euler_create(const az_euler_desc* d, az_euler* out) {
     cudaGetLastError();
     return fail(AZ_ERR_NOMEM, "az_euler_create: control block");
   }
+  ce = cudaMalloc(&e->diag, sizeof(double) * kDiagDoublesPerMember * e->batch);
+  if (ce != cudaSuccess) {
+    cudaFree(e->work);
+    cudaFree(e->ctrl);
+    delete e;
+    cudaGetLastError();
+    return fail(AZ_ERR_NOMEM, "az_euler_create: diagnostics buffer");
+  }
   ce = cudaMemset(e->ctrl, 0, sizeof(Ctrl) * e->batch);
   if (ce != cudaSuccess) {
     cudaFree(e->work);
@@ -259,6 +292,7 @@ az_status az_euler_destroy(az_euler e) {
   if (!e) return AZ_OK;
   cudaFree(e->work);
   cudaFree(e->ctrl);
+  cudaFree(e->diag);
   delete e;
   return AZ_OK;
 }
@@ -276,7 +310,7 @@ static az_status rhs(az_euler e, const void* u, const void* u0, void* out, int m
   const KernelSet* ks = e->ks;
   const long long N = e->N, M = e->M, Nh = e->Nh;
   const unsigned B = unsigned(e->batch);
-  const int nc = ks->tiles.nc;
+  const int nc = ks->tiles[e->v_cols].nc;
   cudaError_t ce;
   if (e->dim == 3) {
     // pass 1: inverse along x with padding, state [3][N][N][Nh] -> A1 [M][N][Nh][3]
@@ -297,7 +331,7 @@ static az_status rhs(az_euler e, const void* u, const void* u0, void* out, int m
     a1.clear_max = 1;
     {
       ProfScope ps(P_INV_X, double(B) * 3 * (N * N * Nh + M * N * Nh) * e->csize, st, e->prof);
-      ce = ks->cols(COLK_PAD_INV, a1, unsigned(a1.ntile), 1, B, st);
+      ce = ks->cols(e->v_cols, COLK_PAD_INV, a1, unsigned(a1.ntile), 1, B, st);
     }
     if (ce != cudaSuccess) return cuda_fail(ce, "rhs pass 1");
     // pass 2: inverse along y with padding, A1 -> A2 [M][M][Nh][3]
@@ -318,7 +352,7 @@ static az_status rhs(az_euler e, const void* u, const void* u0, void* out, int m
     a2.ctrl = e->ctrl;
     {
       ProfScope ps(P_INV_Y, double(B) * 3 * (M * N * Nh + M * M * Nh) * e->csize, st, e->prof);
-      ce = ks->cols(COLK_PAD_INV, a2, unsigned(a2.ntile * M), 1, B, st);
+      ce = ks->cols(e->v_cols, COLK_PAD_INV, a2, unsigned(a2.ntile * M), 1, B, st);
     }
     if (ce != cudaSuccess) return cuda_fail(ce, "rhs pass 2");
     // pass 3: z lines, product, CFL max: A2 -> B1 [M][M][Nh][6]
@@ -336,7 +370,7 @@ static az_status rhs(az_euler e, const void* u, const void* u0, void* out, int m
     r.ctrl = e->ctrl;
     {
       ProfScope ps(P_PRODUCT, double(B) * 9 * (M * M * Nh) * e->csize, st, e->prof);
-      ce = ks->rows_product(3, r, unsigned(cdiv(r.nlines, 2 * ks->tiles.nlp3)), B, st);
+      ce = ks->rows_product(e->v_rows, 3, r, unsigned(cdiv(r.nlines, 2 * ks->tiles[e->v_rows].nlp3)), B, st);
     }
     if (ce != cudaSuccess) return cuda_fail(ce, "rhs pass 3");
   } else {
@@ -358,7 +392,7 @@ static az_status rhs(az_euler e, const void* u, const void* u0, void* out, int m
     a1.clear_max = 1;
     {
       ProfScope ps(P_INV_X, double(B) * 2 * (N * Nh + M * Nh) * e->csize, st, e->prof);
-      ce = ks->cols(COLK_PAD_INV, a1, unsigned(a1.ntile), 1, B, st);
+      ce = ks->cols(e->v_cols, COLK_PAD_INV, a1, unsigned(a1.ntile), 1, B, st);
     }
     if (ce != cudaSuccess) return cuda_fail(ce, "rhs pass 1 (2-D)");
     // pass 2: y lines, product, CFL max: A1 -> B1 [M][Nh][3]
@@ -376,7 +410,7 @@ static az_status rhs(az_euler e, const void* u, const void* u0, void* out, int m
     r.ctrl = e->ctrl;
     {
       ProfScope ps(P_PRODUCT, double(B) * 5 * (M * Nh) * e->csize, st, e->prof);
-      ce = ks->rows_product(2, r, unsigned(cdiv(r.nlines, 2 * ks->tiles.nlp2)), B, st);
+      ce = ks->rows_product(e->v_rows, 2, r, unsigned(cdiv(r.nlines, 2 * ks->tiles[e->v_rows].nlp2)), B, st);
     }
     if (ce != cudaSuccess) return cuda_fail(ce, "rhs pass 2 (2-D)");
   }
@@ -406,7 +440,7 @@ static az_status rhs(az_euler e, const void* u, const void* u0, void* out, int m
     a4.ctrl = e->ctrl;
     {
       ProfScope ps(P_FWD_Y, double(B) * 6 * (M * M * Nh + M * N * Nh) * e->csize, st, e->prof);
-      ce = ks->cols(COLK_TRUNC_FWD, a4, unsigned(a4.ntile * M), 1, B, st);
+      ce = ks->cols(e->v_cols, COLK_TRUNC_FWD, a4, unsigned(a4.ntile * M), 1, B, st);
     }
     if (ce != cudaSuccess) return cuda_fail(ce, "rhs pass 4");
     bsrc = e->buf[0];
@@ -426,7 +460,7 @@ static az_status rhs(az_euler e, const void* u, const void* u0, void* out, int m
   ep.out = out;
   ep.tw = e->tw;
   ep.ninner = ninner;
-  const int ncm = e->dim == 3 ? ks->tiles.ncm3 : ks->tiles.ncm2;
+  const int ncm = e->dim == 3 ? ks->tiles[e->v_epi].ncm3 : ks->tiles[e->v_epi].ncm2;
   ep.ntile = int(cdiv(ninner, ncm));
   ep.N = int(N);
   ep.nh = int(Nh);
@@ -444,7 +478,7 @@ static az_status rhs(az_euler e, const void* u, const void* u0, void* out, int m
     const long long modes = e->dim == 3 ? N * N * Nh : N * Nh;
     const double elems = double(nb) * M * ninner + double(e->dim) * modes * ((mode >= MODE_RK2) ? 3 : 2);
     ProfScope ps(P_EPILOGUE, double(B) * elems * e->csize, st, e->prof);
-    ce = ks->epilogue(e->dim, ep, unsigned(ep.ntile), B, st);
+    ce = ks->epilogue(e->v_epi, e->dim, ep, unsigned(ep.ntile), B, st);
   }
   if (ce != cudaSuccess) return cuda_fail(ce, "rhs epilogue pass");
   return AZ_OK;
@@ -494,6 +528,21 @@ az_status az_euler_dt(az_euler e, double C, void* stream, double* out) {
   }
   for (int b = 0; b < e->batch; ++b)
     if (h[b].err) return fail(AZ_ERR_NONFINITE, "non-finite value in the CFL reduction");
+  return AZ_OK;
+}
+
+az_status az_tune_set(int precision, int L, int kind, int variant) {
+  if ((precision != 0 && precision != 1) || kind < 0 || kind > 5 || (variant != 0 && variant != 1))
+    return fail(AZ_ERR_INVALID, "az_tune_set: bad argument");
+  if (!kernel_set(precision, L)) return fail(AZ_ERR_UNSUPPORTED, "az_tune_set: no compiled length");
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  g_tune[std::make_tuple(precision, L, kind)] = variant;
+  return AZ_OK;
+}
+
+az_status az_tune_get(int precision, int L, int kind, int* variant) {
+  if (!variant || kind < 0 || kind > 5) return fail(AZ_ERR_INVALID, "az_tune_get: bad argument");
+  *variant = tuned_variant(precision, L, kind);
   return AZ_OK;
 }
 
@@ -599,6 +648,11 @@ struct az_sim_s {
   double C;
   void* u = nullptr;
   Ctrl* host = nullptr;  // pinned mirror of the control blocks
+  // One captured SSP-RK3 step.  Every value that changes from step to step
+  // (dt, clock, skip flag, CFL maximum) lives in the device control block, so
+  // the same graph replays every step.
+  cudaGraphExec_t exec = nullptr;
+  bool graph_failed = false;
 };
 
 az_status az_sim_create(az_rk3 ts, double C, const void* u_init, void* stream, az_sim* out) {
@@ -635,6 +689,7 @@ az_status az_sim_create(az_rk3 ts, double C, const void* u_init, void* stream, a
 
 az_status az_sim_destroy(az_sim s) {
   if (!s) return AZ_OK;
+  if (s->exec) cudaGraphExecDestroy(s->exec);
   cudaFree(s->u);
   cudaFreeHost(s->host);
   delete s;
@@ -677,6 +732,48 @@ static az_status sim_step(az_sim s, cudaStream_t st) {
   AZB_CUDA(cudaGetLastError());
   return AZ_OK;
 }
+// Captures one step into a graph (once).  Returns false if the graph is not
+// usable (per-pass profiling is on, or capture failed), in which case the
+// caller launches eagerly.
+static bool sim_graph(az_sim s) {
+  if (g_prof || s->graph_failed) return false;
+  if (s->exec) return true;
+  cudaStream_t cap = nullptr;
+  if (cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    s->graph_failed = true;
+    return false;
+  }
+  cudaGraph_t g = nullptr;
+  bool ok = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+  if (ok) {
+    const az_status st = sim_step(s, cap);
+    const cudaError_t ce = cudaStreamEndCapture(cap, &g);
+    ok = st == AZ_OK && ce == cudaSuccess && g != nullptr;
+  }
+  if (ok) ok = cudaGraphInstantiate(&s->exec, g, 0) == cudaSuccess;
+  if (g) cudaGraphDestroy(g);
+  cudaStreamDestroy(cap);
+  if (!ok) {
+    cudaGetLastError();
+    s->exec = nullptr;
+    s->graph_failed = true;
+  }
+  return ok;
+}
+
+static az_status sim_run_steps(az_sim s, int n, cudaStream_t st) {
+  if (n <= 0) return AZ_OK;
+  if (sim_graph(s)) {
+    for (int i = 0; i < n; ++i) AZB_CUDA(cudaGraphLaunch(s->exec, st));
+    return AZ_OK;
+  }
+  for (int i = 0; i < n; ++i) {
+    az_status r = sim_step(s, st);
+    if (r != AZ_OK) return r;
+  }
+  return AZ_OK;
+}
 }  // namespace azb
 
 az_status az_sim_simulate_until(az_sim s, double t, void* stream) {
@@ -688,10 +785,8 @@ az_status az_sim_simulate_until(az_sim s, double t, void* stream) {
   AZB_CUDA(cudaGetLastError());
   int chunk = 1;
   for (;;) {
-    for (int i = 0; i < chunk; ++i) {
-      az_status r = sim_step(s, st);
-      if (r != AZ_OK) return r;
-    }
+    az_status r = sim_run_steps(s, chunk, st);
+    if (r != AZ_OK) return r;
     AZB_CUDA(cudaMemcpyAsync(s->host, e->ctrl, sizeof(Ctrl) * e->batch, cudaMemcpyDeviceToHost, st));
     AZB_CUDA(cudaStreamSynchronize(st));
     // A member is done once its clock reached t (simulation.cpp:90).
@@ -725,9 +820,167 @@ az_status az_sim_steps(az_sim s, int nsteps, void* stream) {
   const unsigned g = unsigned(cdiv(e->batch, 128));
   k_ctrl_set_tend<<<g, 128, 0, st>>>(e->ctrl, e->batch, INFINITY);
   AZB_CUDA(cudaGetLastError());
-  for (int i = 0; i < nsteps; ++i) {
-    az_status r = sim_step(s, st);
+  return sim_run_steps(s, nsteps, st);
+}
+
+namespace azb {
+__global__ void k_ctrl_member(Ctrl* c, double time, double t_end, int clear_steps) {
+  c->time = time;
+  c->t_end = t_end;
+  c->skip = 0;
+  c->err = 0;
+  c->dt = 0.0;
+  if (clear_steps) c->nsteps = 0;
+}
+}  // namespace azb
+
+az_status az_sim_member_start(az_sim s, int member, const void* u_hat_member, double t_end, void* stream) {
+  if (!s || !u_hat_member) return fail(AZ_ERR_INVALID, "az_sim_member_start: null argument");
+  az_euler e = s->ts->eq;
+  if (member < 0 || member >= e->batch) return fail(AZ_ERR_INVALID, "az_sim_member_start: member out of range");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const size_t bytes = size_t(e->state_mem) * e->csize;
+  AZB_CUDA(cudaMemcpyAsync(static_cast<char*>(s->u) + size_t(member) * bytes, u_hat_member, bytes,
+                           cudaMemcpyDeviceToDevice, st));
+  k_ctrl_member<<<1, 1, 0, st>>>(e->ctrl + member, 0.0, t_end, 1);
+  AZB_CUDA(cudaGetLastError());
+  return AZ_OK;
+}
+
+az_status az_sim_member_stop(az_sim s, int member, void* stream) {
+  if (!s) return fail(AZ_ERR_INVALID, "az_sim_member_stop: null argument");
+  az_euler e = s->ts->eq;
+  if (member < 0 || member >= e->batch) return fail(AZ_ERR_INVALID, "az_sim_member_stop: member out of range");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // A clock past its end makes every kernel of the next steps skip the slot.
+  k_ctrl_member<<<1, 1, 0, st>>>(e->ctrl + member, 1.0, 0.0, 1);
+  AZB_CUDA(cudaGetLastError());
+  return AZ_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Groups: several simulations (any dimension, size or precision) advanced by
+// one captured graph per step, each on its own branch of the graph.
+// ---------------------------------------------------------------------------
+struct az_group_s {
+  std::vector<az_sim> sims;
+  cudaGraphExec_t exec = nullptr;
+};
+
+az_status az_group_create(az_sim* sims, int n, az_group* out) {
+  if (!sims || n < 1 || !out) return fail(AZ_ERR_INVALID, "az_group_create: bad argument");
+  if (g_prof) return fail(AZ_ERR_INVALID, "az_group_create: per-pass profiling must be off while a graph is captured");
+  auto* g = new az_group_s();
+  g->sims.assign(sims, sims + n);
+  for (az_sim s : g->sims)
+    if (!s) {
+      delete g;
+      return fail(AZ_ERR_INVALID, "az_group_create: null simulation");
+    }
+  // Capture: fork one branch per simulation from a root stream, join back.
+  std::vector<cudaStream_t> br(n, nullptr);
+  cudaStream_t root = nullptr;
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> join(n, nullptr);
+  bool ok = cudaStreamCreateWithFlags(&root, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaEventCreateWithFlags(&fork, cudaEventDisableTiming) == cudaSuccess;
+  for (int i = 0; ok && i < n; ++i)
+    ok = cudaStreamCreateWithFlags(&br[i], cudaStreamNonBlocking) == cudaSuccess &&
+         cudaEventCreateWithFlags(&join[i], cudaEventDisableTiming) == cudaSuccess;
+  cudaGraph_t graph = nullptr;
+  az_status step_status = AZ_OK;
+  if (ok) ok = cudaStreamBeginCapture(root, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+  if (ok) {
+    cudaEventRecord(fork, root);
+    for (int i = 0; i < n; ++i) {
+      cudaStreamWaitEvent(br[i], fork, 0);
+      if (step_status == AZ_OK) step_status = sim_step(g->sims[i], br[i]);
+      cudaEventRecord(join[i], br[i]);
+      cudaStreamWaitEvent(root, join[i], 0);
+    }
+    const cudaError_t ce = cudaStreamEndCapture(root, &graph);
+    ok = ce == cudaSuccess && step_status == AZ_OK && graph != nullptr;
+  }
+  if (ok) ok = cudaGraphInstantiate(&g->exec, graph, 0) == cudaSuccess;
+  if (graph) cudaGraphDestroy(graph);
+  for (int i = 0; i < n; ++i) {
+    if (br[i]) cudaStreamDestroy(br[i]);
+    if (join[i]) cudaEventDestroy(join[i]);
+  }
+  if (fork) cudaEventDestroy(fork);
+  if (root) cudaStreamDestroy(root);
+  if (!ok) {
+    const cudaError_t last = cudaGetLastError();
+    delete g;
+    if (step_status != AZ_OK) return step_status;
+    return fail(AZ_ERR_CUDA, std::string("az_group_create: graph capture failed: ") + cudaGetErrorString(last));
+  }
+  *out = g;
+  return AZ_OK;
+}
+
+az_status az_group_destroy(az_group g) {
+  if (!g) return AZ_OK;
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  delete g;
+  return AZ_OK;
+}
+
+az_status az_group_steps(az_group g, int nsteps, void* stream) {
+  if (!g || nsteps < 0) return fail(AZ_ERR_INVALID, "az_group_steps: bad argument");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  for (int i = 0; i < nsteps; ++i) AZB_CUDA(cudaGraphLaunch(g->exec, st));
+  return AZ_OK;
+}
+
+az_status az_group_set_end(az_group g, double t, void* stream) {
+  if (!g) return fail(AZ_ERR_INVALID, "az_group_set_end: null argument");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  for (az_sim s : g->sims) {
+    az_euler e = s->ts->eq;
+    k_ctrl_set_tend<<<unsigned(cdiv(e->batch, 128)), 128, 0, st>>>(e->ctrl, e->batch, t);
+    AZB_CUDA(cudaGetLastError());
+  }
+  return AZ_OK;
+}
+
+az_status az_group_simulate_until(az_group g, double t, void* stream) {
+  if (!g) return fail(AZ_ERR_INVALID, "az_group_simulate_until: null argument");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  az_status r = az_group_set_end(g, t, stream);
+  if (r != AZ_OK) return r;
+  int chunk = 1;
+  for (;;) {
+    r = az_group_steps(g, chunk, stream);
     if (r != AZ_OK) return r;
+    double min_left = INFINITY;
+    bool any = false;
+    for (az_sim s : g->sims) {
+      az_euler e = s->ts->eq;
+      AZB_CUDA(cudaMemcpyAsync(s->host, e->ctrl, sizeof(Ctrl) * e->batch, cudaMemcpyDeviceToHost, st));
+    }
+    AZB_CUDA(cudaStreamSynchronize(st));
+    for (az_sim s : g->sims) {
+      az_euler e = s->ts->eq;
+      for (int b = 0; b < e->batch; ++b) {
+        if (s->host[b].err) return fail(AZ_ERR_NONFINITE, "non-finite value in the CFL reduction");
+        if (s->host[b].time < t) {
+          any = true;
+          const double dt = s->host[b].dt;
+          const double left = dt > 0 ? (t - s->host[b].time) / dt : 1.0;
+          if (left < min_left) min_left = left;
+        }
+      }
+    }
+    if (!any) break;
+    chunk = int(std::floor(min_left * 0.9));
+    if (chunk < 1) chunk = 1;
+    if (chunk > 64) chunk = 64;
+  }
+  for (az_sim s : g->sims) {
+    az_euler e = s->ts->eq;
+    k_ctrl_finish<<<unsigned(cdiv(e->batch, 128)), 128, 0, st>>>(e->ctrl, e->batch, t);
+    AZB_CUDA(cudaGetLastError());
   }
   return AZ_OK;
 }
@@ -884,7 +1137,8 @@ static az_status fft_axis(az_fft f, int ax, const void* in, void* out, int kind,
   c.out = out;
   c.tw = f->tw[ax];
   c.ninner = inner;
-  c.ntile = int(cdiv(inner, ks->tiles.nc));
+  const int v = tuned_variant(f->prec, int(rows), 0);
+  c.ntile = int(cdiv(inner, ks->tiles[v].nc));
   c.n_short = int(rows);
   c.in_row = inner;
   c.out_row = inner;
@@ -903,7 +1157,7 @@ static az_status fft_axis(az_fft f, int ax, const void* in, void* out, int kind,
     cc.out_comp = rows * inner;
     cc.in_outer = 0;
     cc.out_outer = 0;
-    cudaError_t ce = ks->cols(kind, cc, unsigned(cc.ntile), unsigned(chunk), 1, st);
+    cudaError_t ce = ks->cols(v, kind, cc, unsigned(cc.ntile), unsigned(chunk), 1, st);
     if (ce != cudaSuccess) return cuda_fail(ce, "fft column pass");
     done += chunk;
   }
@@ -925,7 +1179,8 @@ az_status az_fft_forward(az_fft f, void* stream) {
   r.nlines = lines;
   r.in_line = f->shape[last];
   r.out_line = f->nh;
-  cudaError_t ce = f->ks[last]->r2c(r, unsigned(cdiv(lines, 2 * f->ks[last]->tiles.nlpr)), st);
+  const int v = tuned_variant(f->prec, int(f->shape[last]), 1);
+  cudaError_t ce = f->ks[last]->r2c(v, r, unsigned(cdiv(lines, 2 * f->ks[last]->tiles[v].nlpr)), st);
   if (ce != cudaSuccess) return cuda_fail(ce, "fft r2c pass");
   for (int ax = last - 1; ax >= f->dim - f->nt; --ax) {
     az_status s = fft_axis(f, ax, f->u_hat, f->u_hat, COLK_PLAIN_FWD, st);
@@ -954,7 +1209,8 @@ az_status az_fft_backward(az_fft f, void* stream) {
   r.nlines = lines;
   r.in_line = f->nh;
   r.out_line = f->shape[last];
-  cudaError_t ce = f->ks[last]->c2r(r, unsigned(cdiv(lines, 2 * f->ks[last]->tiles.nlpr)), st);
+  const int v = tuned_variant(f->prec, int(f->shape[last]), 1);
+  cudaError_t ce = f->ks[last]->c2r(v, r, unsigned(cdiv(lines, 2 * f->ks[last]->tiles[v].nlpr)), st);
   if (ce != cudaSuccess) return cuda_fail(ce, "fft c2r pass");
   return AZ_OK;
 }

@@ -27,7 +27,12 @@ struct az_euler_s {
   double norm;
   double Md;
   bool prof = true;  // false: never record per-pass timing events
+  int v_cols = 0, v_rows = 0, v_epi = 0;  // plan variants of the three pass kinds
+  double* diag = nullptr;  // partial sums of the energy / enstrophy reduction
 };
+
+// Doubles of az_euler_s::diag per member.
+constexpr int kDiagDoublesPerMember = 512 * 2 + 2;
 
 
 namespace azb {
@@ -38,4 +43,7 @@ az_status euler_dudt_launch(az_euler e, void* dudt_hat, const void* u_hat, cudaS
 az_status set_error(az_status st, const char* msg);
 // Compiled kernels of one (precision, transform length), or nullptr.
 const KernelSet* find_kernel_set(int precision, int L);
+// Plan variant (0 std, 1 wide) the tuning table holds for a pass kind
+// (0 column passes, 1 product pass, 2 epilogue pass).
+int tuned_variant(int precision, int L, int kind);
 }  // namespace azb

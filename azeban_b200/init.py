@@ -76,3 +76,30 @@ def double_shear_layer(N: int, rho: float, delta: float, phases, precision: str 
     v = delta * torch.sin(2 * math.pi * x[None] + ph[:, None, None])
     field = torch.stack([u[None].expand_as(v), v], dim=1)
     return spectral(field.to(_RDT[precision]).contiguous())
+
+
+def fractional_brownian(dim: int, N: int, hurst: float = 0.75, seed: int = 0, precision: str = "f64") -> torch.Tensor:
+    """Random divergence-free field: Gaussian Fourier coefficients with
+    amplitude |n|^-(H + d/2), Leray-projected, normalised to kinetic energy
+    1/2 <|u|^2> = 1.  The coefficients come from the forward transform of
+    seeded Gaussian white noise, so the spectrum is Hermitian-consistent.
+    [dim, N, ..., N/2+1].  (azeban's own BrownianMotion,
+    src/azeban/init/brownian_motion.cpp:144-203, draws uniform coefficients;
+    this is the Gaussian form of the workloads.)"""
+    gen = torch.Generator(device="cuda").manual_seed(int(seed))
+    noise = torch.randn((dim,) + (N,) * dim, generator=gen, device="cuda", dtype=torch.float64)
+    u_hat = spectral(noise.to(_RDT[precision]), project=False)
+    idx = torch.arange(N, device="cuda", dtype=torch.float64)
+    signed = torch.where(idx >= N // 2 + 1, idx - N, idx)
+    axes = [signed] * (dim - 1) + [torch.arange(N // 2 + 1, device="cuda", dtype=torch.float64)]
+    k2 = sum(g * g for g in torch.meshgrid(*axes, indexing="ij"))
+    amp = torch.where(k2 > 0, k2.clamp_min(1e-300) ** (-(hurst + dim / 2.0) / 2.0), torch.zeros_like(k2))
+    u_hat = u_hat * amp.to(u_hat.real.dtype)
+    leray(u_hat)
+    # kinetic energy of the unnormalised half spectrum (Parseval)
+    w = torch.full((N // 2 + 1,), 2.0, device="cuda", dtype=torch.float64)
+    w[0] = 1.0
+    if N % 2 == 0:
+        w[N // 2] = 1.0
+    e = 0.5 * (w * (u_hat.abs().to(torch.float64) ** 2)).sum() / float(N) ** (2 * dim)
+    return (u_hat / torch.sqrt(e).to(u_hat.real.dtype)).contiguous()

@@ -97,6 +97,15 @@ double az_euler_visc(az_euler eq);
 /* Bytes of device workspace the equation holds. */
 size_t az_euler_workspace_size(az_euler eq);
 
+/* Kinetic energy 1/2 <|u|^2> and enstrophy 1/2 <|curl u|^2> of every member
+ * of u_hat (host arrays of length batch), summed in FP64 with compensated
+ * sums in a fixed order, for any precision of the solve.  No counterpart in
+ * this form in the reference, which writes spectra of these quantities
+ * (src/azeban/operations/energy_spectrum.cpp, enstrophy_spectrum.cpp).
+ * Synchronises the stream. */
+az_status az_euler_diagnostics(az_euler eq, const void* u_hat, void* stream, double* energy,
+                               double* enstrophy);
+
 /* ---- TimeIntegrator<Dim> / SSP_RK3<Dim> (include/azeban/evolution/time_integrator.hpp:30-60,
  *      include/azeban/evolution/ssp_rk3.hpp:28-76) ---------------------- */
 
@@ -131,6 +140,34 @@ void* az_sim_u(az_sim sim);
  * Any pointer may be NULL.  Synchronises the stream. */
 az_status az_sim_state(az_sim sim, void* stream, double* time, long long* nsteps, double* dt);
 
+/* One member (slot) of a batched simulation, for continuous batching (no
+ * counterpart in the reference, whose closest is the per-sample loop of
+ * src/azeban/run_from_config.cpp:81-102).  member_start copies a state into
+ * the slot and restarts its clock at 0 with end t_end; the slot then steps
+ * with every step of the simulation (or of a group holding it) until its
+ * clock reaches t_end, and is skipped afterwards.  member_stop frees the slot
+ * (it is skipped until started again). */
+az_status az_sim_member_start(az_sim sim, int member, const void* u_hat_member, double t_end,
+                              void* stream);
+az_status az_sim_member_stop(az_sim sim, int member, void* stream);
+
+/* ---- groups of simulations (no counterpart in the reference) ------------ */
+
+typedef struct az_group_s* az_group;
+
+/* Several simulations of any dimension, size and precision advanced together:
+ * one SSP-RK3 step of all of them is captured once as a graph with one branch
+ * per simulation, so their work overlaps on the device.  The simulations must
+ * outlive the group. */
+az_status az_group_create(az_sim* sims, int n, az_group* out);
+az_status az_group_destroy(az_group g);
+/* nsteps graph launches; a member whose clock reached its end is skipped. */
+az_status az_group_steps(az_group g, int nsteps, void* stream);
+/* Sets every member's end to t (no step). */
+az_status az_group_set_end(az_group g, double t, void* stream);
+/* simulate_until for every member of every simulation of the group. */
+az_status az_group_simulate_until(az_group g, double t, void* stream);
+
 /* ---- FFT<Dim> (include/azeban/operations/fft.hpp:37-121,
  *      make_fft src/azeban/operations/fft_factory.cpp:10-48) ----------- */
 
@@ -155,6 +192,17 @@ az_status az_fft_forward(az_fft fft, void* stream);
 az_status az_fft_backward(az_fft fft, void* stream);
 /* FFT::get_work_area_size (fft.hpp:93). */
 size_t az_fft_work_area_size(az_fft fft);
+
+/* ---- tuning table (no reference counterpart; the reference's nearest is
+ *      optimal_fft_size reading a benchmark file, src/azeban/operations/fft.cpp:63-108) */
+
+/* Plan variant (0: at most 24 elements per thread; 1: wide, fewer shared-
+ * memory exchanges) used for transform length L of a precision by one pass
+ * kind: 0 column passes, 1 contiguous-axis passes, 2 epilogue pass of 3-D
+ * solves (and of FFT<Dim>), 3-5 the same of 2-D solves.  Applies to solves
+ * and FFTs created afterwards. */
+az_status az_tune_set(int precision, int L, int kind, int variant);
+az_status az_tune_get(int precision, int L, int kind, int* variant);
 
 /* ---- per-pass timing (no reference counterpart; replaces the reference's
  *      Profiler, include/azeban/profiler.hpp:35-135, for the transform passes) */

@@ -582,3 +582,25 @@ def rel_l2(a: np.ndarray, b: np.ndarray) -> float:
     """||a - b||_2 / ||b||_2 over the flat arrays."""
     nb = np.linalg.norm(np.ravel(b))
     return float(np.linalg.norm(np.ravel(a - b)) / (nb if nb > 0 else 1.0))
+
+
+# --------------------------------------------------------------------------
+# Diagnostics (Parseval on the half spectrum; exact-rounded sums)
+# --------------------------------------------------------------------------
+
+def energy_enstrophy(u_hat: np.ndarray):
+    """1/2 <|u|^2> and 1/2 <|curl u|^2> of one unnormalised r2c spectrum
+    [d, N, (N,) N/2+1], summed with math.fsum (correctly rounded)."""
+    d = u_hat.ndim - 1
+    N = u_hat.shape[1]
+    kk = [2 * PI * signed_index(N).astype(np.float64)] * (d - 1) + [
+        2 * PI * np.arange(u_hat.shape[-1], dtype=np.float64)]
+    ks = np.meshgrid(*kk, indexing="ij")
+    k2 = sum(k * k for k in ks)
+    last = np.arange(u_hat.shape[-1])
+    w = np.where((last == 0) | (2 * last == N), 1.0, 2.0)
+    a2 = sum(np.abs(u_hat[c]) ** 2 for c in range(d))
+    scale = 1.0 / float(N) ** (2 * d)
+    e = 0.5 * scale * math.fsum((w * a2).ravel())
+    z = 0.5 * scale * math.fsum((w * k2 * a2).ravel())
+    return e, z

@@ -236,3 +236,25 @@ def test_unsupported_padding_raises():
     g = az.Grid(2, 16, 20)
     with pytest.raises(az.AzebanError):
         az.IncompressibleEuler(g, az.make_viscosity(VISC_CFGS["smooth"], g))
+
+
+@pytest.mark.parametrize("dim,N,prec,batch", [(2, 64, "f64", 1), (3, 32, "f64", 3), (3, 32, "f32", 2), (2, 128, "f32", 4)])
+def test_energy_enstrophy_fp64_sums(dim, N, prec, batch):
+    """FP64 compensated diagnostics equal correctly rounded sums; a member's
+    value is the same alone and inside a batch."""
+    g = az.Grid(dim, N)
+    v = az.make_viscosity(VISC_CFGS["smooth"], g)
+    fields = [random_field_hat(dim, N, seed=70 + b) for b in range(batch)]
+    eq = az.IncompressibleEuler(g, v, prec, batch=batch)
+    dev = to_dev(np.stack(fields) if batch > 1 else fields[0], prec)
+    E, W = eq.diagnostics(dev)
+    E = E if batch > 1 else [E]
+    W = W if batch > 1 else [W]
+    for b in range(batch):
+        rounded = to_host(dev[b] if batch > 1 else dev)
+        e_ref, w_ref = ora.energy_enstrophy(rounded)
+        assert abs(E[b] - e_ref) <= 1e-14 * e_ref
+        assert abs(W[b] - w_ref) <= 1e-14 * w_ref
+        alone = az.IncompressibleEuler(g, v, prec)
+        e1, w1 = alone.diagnostics(to_dev(fields[b], prec))
+        assert e1 == E[b] and w1 == W[b]
