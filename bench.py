@@ -52,6 +52,11 @@ def parse():
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workload", default="tg3d256",
+                    choices=["tg3d256", "tg2d64", "tg3d-accuracy", "dsl-ensemble", "fbm512", "serving"],
+                    help="tg3d256 is the headline; the others are the remaining workloads, one JSON line each")
+    ap.add_argument("--duration", type=float, default=60.0, help="serving: seconds of Poisson arrivals")
+    ap.add_argument("--rate", type=float, default=200.0, help="serving: arrivals per second")
     return ap.parse_args()
 
 
@@ -375,11 +380,241 @@ def run_ours(args, rank, world, local):
         dist.destroy_process_group()
 
 
+def _ev():
+    import torch
+    return torch.cuda.Event(enable_timing=True)
+
+
+def run_tg2d64(args):
+    """Taylor-Green 2-D 64^2 FP64 to t = 1 (the reference's CPU-runnable
+    configuration): GPU time to solution, the oracle's time on the host cores,
+    and their agreement."""
+    import torch
+
+    import azeban_b200 as az
+    from azeban_b200 import init as azinit
+    from oracle import euler_oracle as ora
+    g = az.Grid(2, 64)
+    sim = az.Simulation(g, C_CFL, az.SSP_RK3(az.IncompressibleEuler(g, az.make_viscosity(VISC_CFG, g))),
+                        azinit.taylor_green(2, 64, "f64"))
+    torch.cuda.synchronize()
+    e0, e1 = _ev(), _ev()
+    e0.record()
+    sim.simulate_until(1.0)
+    e1.record()
+    torch.cuda.synchronize()
+    gpu_ms = e0.elapsed_time(e1)
+    og = ora.Grid(2, 64)
+    ora.set_workers(os.cpu_count() or 1)
+    t0 = time.perf_counter()
+    osim = ora.Simulation(og, C_CFL, ora.SSP_RK3(ora.IncompressibleEuler(og, ora.make_viscosity(VISC_CFG, og))),
+                          ora.initialize(ora.taylor_green_workload(2, 64)))
+    osim.simulate_until(1.0)
+    cpu_s = time.perf_counter() - t0
+    steps = sim.state()[1][0]
+    print(json.dumps({"workload": "TG-2D 64^2 FP64 to t=1", "steps": steps, "oracle_steps": len(osim.dts),
+                      "gpu_ms_to_solution": gpu_ms, "cpu_oracle_s_to_solution": cpu_s,
+                      "cpu_cores": os.cpu_count(),
+                      "l2_rel_gpu_vs_oracle": ora.rel_l2(sim.u().cpu().numpy(), osim.u_)}), flush=True)
+
+
+def run_tg3d_accuracy(args):
+    """Taylor-Green 3-D at 128^3 and 256^3, FP64 and FP32 bulk: relative L2 of
+    FP32 vs FP64 at 10 output times over [0, 1/(2 pi)] (t in [0, 1] on
+    [0, 2 pi)^3) and at azeban t = 1, with the FP64 rounded-initial-state floor."""
+    import torch
+
+    import azeban_b200 as az
+    from azeban_b200 import init as azinit
+    out = []
+    for N in (128, 256):
+        g = az.Grid(3, N)
+        v = az.make_viscosity(VISC_CFG, g)
+        u64 = azinit.taylor_green(3, N, "f64")
+        u32 = azinit.taylor_green(3, N, "f32")
+        sims = {"fp32": az.Simulation(g, C_CFL, az.SSP_RK3(az.IncompressibleEuler(g, v, "f32")), u32),
+                "fp64": az.Simulation(g, C_CFL, az.SSP_RK3(az.IncompressibleEuler(g, v, "f64")), u64),
+                "floor": az.Simulation(g, C_CFL, az.SSP_RK3(az.IncompressibleEuler(g, v, "f64")),
+                                       u32.to(torch.complex128).contiguous())}
+        times = [(i + 1) / (10 * 2 * math.pi) for i in range(10)] + [1.0]
+        rows = []
+        for t in times:
+            for s_ in sims.values():
+                s_.simulate_until(t)
+            ref = sims["fp64"].u()
+            nrm = torch.linalg.vector_norm(ref)
+            rows.append({"t": t, "l2_fp32_vs_fp64": float(torch.linalg.vector_norm(sims["fp32"].u().to(torch.complex128) - ref) / nrm),
+                         "floor": float(torch.linalg.vector_norm(sims["floor"].u() - ref) / nrm)})
+        out.append({"N": N, "outputs": rows})
+        del sims
+    print(json.dumps({"workload": "TG-3D accuracy FP32 bulk vs FP64", "results": out}), flush=True)
+
+
+def run_dsl_ensemble(args):
+    """2-D double-shear-layer ensemble, 512 members of mixed resolution in one
+    graph per step (128^2 x256, 256^2 x192, 512^2 x64), FP32 bulk, phases
+    phi ~ U[0, 2 pi) from a seed, to t = 1/(2 pi) (t = 1 on [0, 2 pi)^2)."""
+    import numpy as np
+    import torch
+
+    import azeban_b200 as az
+    from azeban_b200 import init as azinit
+    classes = [(128, 256), (256, 192), (512, 64)]
+    rng = np.random.default_rng(2024)
+    sims, keep, first = [], [], {}
+    for N, B in classes:
+        g = az.Grid(2, N)
+        eq = az.IncompressibleEuler(g, az.make_viscosity(VISC_CFG, g), "f32", batch=B)
+        ts = az.SSP_RK3(eq)
+        phases = rng.uniform(0, 2 * math.pi, B)
+        u0 = azinit.double_shear_layer(N, math.pi / 15, 0.05, phases, "f32")
+        sims.append(az.Simulation(g, C_CFL, ts, u0))
+        keep += [eq, ts]
+        first[N] = (phases[0], u0[0].clone())
+    group = az.Group(sims)
+    t_end = 1.0 / (2 * math.pi)
+    torch.cuda.synchronize()
+    e0, e1 = _ev(), _ev()
+    e0.record()
+    group.simulate_until(t_end)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    msteps = sum(sum(s.state()[1]) for s in sims)
+    errs = {}
+    for (N, B), sim in zip(classes, sims):
+        g = az.Grid(2, N)
+        ph, _ = first[N]
+        u64 = azinit.double_shear_layer(N, math.pi / 15, 0.05, [ph], "f64")[0]
+        ref = az.Simulation(g, C_CFL, az.SSP_RK3(az.IncompressibleEuler(g, az.make_viscosity(VISC_CFG, g), "f64")), u64)
+        ref.simulate_until(t_end)
+        r = ref.u()
+        errs[f"{N}^2"] = float(torch.linalg.vector_norm(sim.u()[0].to(torch.complex128) - r) / torch.linalg.vector_norm(r))
+    print(json.dumps({"workload": "DSL-2D ensemble 512 members (128^2 x256, 256^2 x192, 512^2 x64) FP32, one graph per step",
+                      "t_end": t_end, "wall_ms": ms, "member_steps": msteps,
+                      "member_steps_per_s": msteps / (ms / 1e3), "l2_member0_vs_fp64": errs}), flush=True)
+
+
+def run_fbm512(args):
+    """3-D 512^3 (768^3 padded) fractional Brownian field, H = 0.75, FP32 bulk,
+    50 steps: per-pass HBM GB/s, and the error vs an FP64 run of the same
+    initial state at 512^3 and vs FP64 at 256^3 from the truncated state."""
+    import ctypes as ct
+
+    import torch
+
+    import azeban_b200 as az
+    from azeban_b200 import _lib
+    from azeban_b200 import init as azinit
+    N, steps = 512, 50
+    g = az.Grid(3, N)
+    v = az.make_viscosity(VISC_CFG, g)
+    u64 = azinit.fractional_brownian(3, N, 0.75, seed=7, precision="f64")
+    u32 = u64.to(torch.complex64).contiguous()
+    sim = az.Simulation(g, C_CFL, az.SSP_RK3(az.IncompressibleEuler(g, v, "f32")), u32)
+    torch.cuda.synchronize()
+    _lib.lib.az_profile_enable(1)
+    e0, e1 = _ev(), _ev()
+    e0.record()
+    sim.steps(steps)
+    e1.record()
+    torch.cuda.synchronize()
+    _lib.lib.az_profile_enable(0)
+    ms = (ct.c_double * 5)()
+    by = (ct.c_double * 5)()
+    nl = (ct.c_longlong * 5)()
+    _lib.check(_lib.lib.az_profile_read(ms, by, nl, 5))
+    names = ["inv_x_pad", "inv_y_pad", "z_product", "fwd_y_trunc", "fwd_x_epilogue"]
+    passes = {n: {"avg_ms": ms[i] / nl[i], "gbs": by[i] / nl[i] / (ms[i] / nl[i] * 1e-3) / 1e9}
+              for i, n in enumerate(names) if nl[i]}
+    t_reached = sim.state()[0][0]
+    u_fp32 = sim.u().clone()
+    del sim
+    ref = az.Simulation(g, C_CFL, az.SSP_RK3(az.IncompressibleEuler(g, v, "f64")), u64)
+    ref.simulate_until(t_reached)
+    r = ref.u()
+    err512 = float(torch.linalg.vector_norm(u_fp32.to(torch.complex128) - r) / torch.linalg.vector_norm(r))
+    del ref, r
+    # FP64 at 256^3 from the truncated initial state, compared on the retained modes
+    Nc = 256
+    idx = torch.cat([torch.arange(0, Nc // 2 + 1), torch.arange(N - Nc // 2 + 1, N)]).cuda()
+    def trunc(a):
+        return a.index_select(1, idx).index_select(2, idx)[..., : Nc // 2 + 1] * (Nc / N) ** 3
+    gc = az.Grid(3, Nc)
+    refc = az.Simulation(gc, C_CFL, az.SSP_RK3(az.IncompressibleEuler(gc, az.make_viscosity(VISC_CFG, gc), "f64")),
+                         trunc(u64).contiguous())
+    refc.simulate_until(t_reached)
+    rc = refc.u()
+    err256 = float(torch.linalg.vector_norm(trunc(u_fp32.to(torch.complex128)) - rc) / torch.linalg.vector_norm(rc))
+    print(json.dumps({"workload": "fBm-3D 512^3 FP32 bulk, 50 steps", "ms_per_step": e0.elapsed_time(e1) / steps,
+                      "member_steps_per_s": steps / (e0.elapsed_time(e1) / 1e3), "t_reached": t_reached,
+                      "passes": passes, "l2_vs_fp64_512": err512, "l2_vs_fp64_256_truncated": err256}), flush=True)
+
+
+def run_serving(args):
+    """Poisson arrivals (default 200/s for 60 s) of 2-D double-shear-layer and
+    3-D fBm solves, N from {64^2..512^2} and {64^3..256^3} with probability
+    proportional to 1/cost, t_end ~ U[0.25, 1]; continuous batching with slots
+    sized from an HBM budget.  Beside it, the FP64 one-at-a-time baseline:
+    each class's FP64 solve time measured alone, and the same arrivals served
+    first-in first-out one at a time with those service times."""
+    import numpy as np
+    import torch
+
+    import azeban_b200 as az
+    from azeban_b200 import serving
+    reqs = serving.poisson_stream(args.rate, args.duration, seed=11)
+    free, _ = torch.cuda.mem_get_info()
+    weights = {c: 1.0 for c in serving.CLASSES}
+    for c in [(2, 64), (2, 128)]:
+        weights[c] = 4.0
+    caps = serving.plan_capacities(int(free * 0.5), "f32", weights)
+    caps = {c: min(k, 256) for c, k in caps.items()}
+    loop = serving.ServingLoop(caps, "f32")
+    records, stats, _ = loop.run(reqs)
+    # FP64 one at a time: per-class solve time at the mean t_end, measured alone
+    per_class = {}
+    for c in serving.CLASSES:
+        sub = [r for r in reqs if (r.dim, r.N) == c]
+        if not sub:
+            continue
+        r0 = sub[0]
+        g = az.Grid(c[0], c[1])
+        u0 = serving.initial_state(r0, "f64")
+        sim = az.Simulation(g, 0.2, az.SSP_RK3(az.IncompressibleEuler(g, az.make_viscosity(serving.VISC, g), "f64")), u0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sim.simulate_until(r0.t_end)
+        torch.cuda.synchronize()
+        per_class[c] = (time.perf_counter() - t0) / r0.t_end
+    clock, lat, busy = 0.0, [], 0.0
+    for r in sorted(reqs):
+        svc = per_class[(r.dim, r.N)] * r.t_end
+        clock = max(clock, r.arrival) + svc
+        busy += svc
+        lat.append(clock - r.arrival)
+    base = {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+            "makespan_s": clock, "busy_s": busy}
+    print(json.dumps({"workload": f"serving Poisson {args.rate}/s for {args.duration}s, FP32 bulk continuous batching",
+                      "capacities": {f"{d}D-{n}": k for (d, n), k in caps.items()}, "stats": stats,
+                      "fp64_one_at_a_time": base,
+                      "fp64_class_seconds_per_unit_time": {f"{d}D-{n}": v for (d, n), v in per_class.items()}}),
+          flush=True)
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    extra = {"tg2d64": run_tg2d64, "tg3d-accuracy": run_tg3d_accuracy, "dsl-ensemble": run_dsl_ensemble,
+             "fbm512": run_fbm512, "serving": run_serving}
+    if args.workload in extra:
+        import torch
+        torch.cuda.set_device(local)
+        if rank == 0:
+            extra[args.workload](args)
         return
     run_ours(args, rank, world, local)
 
