@@ -17,7 +17,8 @@ struct alignas(64) Ctrl {
   double t_end;               // target of simulate_until
   double max_dt;              // min(t_end - time, viscous cap) of this step
   long long nsteps;           // completed steps
-  int err;                    // bit 0: non-finite value met in the CFL reduction
+  int err;                    // bit 0: non-finite value met in the CFL reduction;
+                              // bit 1: a bounded wait on a bulk copy ran out
   int pad_;
 };
 

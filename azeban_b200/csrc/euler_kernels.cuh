@@ -93,16 +93,19 @@ __global__ void __launch_bounds__(NC * Plan<L, V>::TPL) k_cols(ColArgs a) {
   load_twiddles<C, L>(tw, reinterpret_cast<const C*>(a.tw));
   __syncthreads();
   const int n = a.n_short;
+  // Row offsets fit 32 bits (the launcher checks L * stride < 2^31).
+  const int in_row = int(a.in_row);
+  const int out_row = int(a.out_row);
   auto load = [&](int m) -> C {
     int src = m;
     if constexpr (MODE == COL_PAD) src = pad_src_row(m, n, L);
     if (!valid || src < 0) return cmk<C>(T(0), T(0));
-    return in[src * a.in_row];
+    return in[src * in_row];
   };
   auto store = [&](int m, C v) {
     int dst = m;
     if constexpr (MODE == COL_TRUNC) dst = retained_row(m, n, L);
-    if (valid && dst >= 0) out[dst * a.out_row] = v;
+    if (valid && dst >= 0) out[dst * out_row] = v;
   };
   fft_columns<C, S, L, NC, false, P>(sm, tw, col, tl, load, store);
 }
@@ -388,9 +391,10 @@ __global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NCM * Plan<L, V>::TPL)
     const long long p = (long long)tile * NCM + pl;
     const bool valid = p < a.ninner;
     const C* Bp = reinterpret_cast<const C*>(a.B) + member * a.B_mem + (long long)tile * NC + col;
+    const int B_row = int(a.B_row);  // L * B_row < 2^31, checked by the launcher
     fft_columns<C, -1, L, SROW, true, P>(
         sm, tw, col, tl,
-        [&](int m) -> C { return valid ? Bp[m * a.B_row] : cmk<C>(T(0), T(0)); },
+        [&](int m) -> C { return valid ? Bp[m * B_row] : cmk<C>(T(0), T(0)); },
         [&](int m, C v) {
           const int i = retained_row(m, N, L);
           if (i >= 0) sm[i * SROW + col] = v;
@@ -404,19 +408,20 @@ __global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NCM * Plan<L, V>::TPL)
   const C* u = reinterpret_cast<const C*>(a.u) + member * a.u_mem;
   const C* u0 = reinterpret_cast<const C*>(a.u0) + member * a.u_mem;
   C* out = reinterpret_cast<C*>(a.out) + member * a.u_mem;
+  const int u_row = int(a.u_row), u_comp = int(a.u_comp);  // a member's state < 2^31 elements
   for (int idx = tid; idx < N * NCM; idx += NT) {
     const int pl = idx % NCM;
     const int i = idx / NCM;
-    const long long p = (long long)tile * NCM + pl;
+    const int p = tile * NCM + pl;
     if (p >= a.ninner) continue;
     const int i_ = i >= N / 2 + 1 ? i - N : i;
     C Bv[NB];
 #pragma unroll
     for (int c = 0; c < NB; ++c) Bv[c] = sm[i * SROW + pl * NB + c];
-    const long long off = (long long)i * a.u_row + p;
+    const int off = i * u_row + p;
     C uv[DIM];
 #pragma unroll
-    for (int c = 0; c < DIM; ++c) uv[c] = u[c * a.u_comp + off];
+    for (int c = 0; c < DIM; ++c) uv[c] = u[c * u_comp + off];
     C Lh[DIM];
     T absk2;
     if constexpr (DIM == 2) {
@@ -433,8 +438,8 @@ __global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NCM * Plan<L, V>::TPL)
       Lh[0] = cmk<C>(c11 * b1.x + c12 * b2.x, c11 * b1.y + c12 * b2.y);
       Lh[1] = cmk<C>(c12 * b1.x + c22 * b2.x, c12 * b1.y + c22 * b2.y);
     } else {
-      const int j = (int)(p / a.nh);
-      const int kk = (int)(p % a.nh);
+      const int j = p / a.nh;
+      const int kk = p - j * a.nh;
       const int j_ = j >= N / 2 + 1 ? j - N : j;
       const T k1 = twopi * T(i_);
       const T k2 = twopi * T(j_);
@@ -470,7 +475,7 @@ __global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NCM * Plan<L, V>::TPL)
         if (a.mode == MODE_RK1) {
           r = t;
         } else {
-          const C w = u0[c * a.u_comp + off];
+          const C w = u0[c * u_comp + off];
           if (a.mode == MODE_RK2) {
             r = cmk<C>(T(0.75) * w.x + T(0.25) * t.x, T(0.75) * w.y + T(0.25) * t.y);
           } else {
@@ -479,7 +484,7 @@ __global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NCM * Plan<L, V>::TPL)
           }
         }
       }
-      out[c * a.u_comp + off] = r;
+      out[c * u_comp + off] = r;
     }
   }
 }

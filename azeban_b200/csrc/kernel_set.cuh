@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include "euler_kernels.cuh"
+#include "zpass.cuh"
 
 namespace azb {
 
@@ -26,9 +27,12 @@ struct TileShape {
 struct KernelSet {
   int L;
   int precision;  // 0 FP64, 1 FP32
-  TileShape tiles[2];  // per plan variant
+  TileShape tiles[2];  // per plan variant (bit 0 of a variant number)
   cudaError_t (*cols)(int v, int kind, const ColArgs&, unsigned gx, unsigned gy, unsigned gz, cudaStream_t);
   cudaError_t (*rows_product)(int v, int dim, const RowArgs&, unsigned gx, unsigned gy, cudaStream_t);
+  // Bulk-copy form of the product pass: plan variant v & 1; v & 4 selects the
+  // persistent, double-buffered launch.
+  cudaError_t (*zpass)(int v, int dim, const ZArgs&, cudaStream_t);
   cudaError_t (*epilogue)(int v, int dim, const EpiArgs&, unsigned gx, unsigned gy, cudaStream_t);
   cudaError_t (*c2r)(int v, const RealRowArgs&, unsigned gx, cudaStream_t);
   cudaError_t (*r2c)(int v, const RealRowArgs&, unsigned gx, cudaStream_t);
@@ -49,6 +53,20 @@ template <typename T, int L, int V> struct Tiles {
   static constexpr int NCM3 = kclamp(kpow2floor(81920 / (L * 6 * CB)), 1, 16);
   static constexpr int NCM2 = kclamp(kpow2floor(81920 / (L * 3 * CB)), 1, 16);
   static constexpr int NLPR = kclamp(kpow2floor(49152 / (L * CB)), 1, 64);
+};
+
+// Line pairs per chunk of k_zpass: about 40 KB of work area, raised until the
+// CTA's thread count is a whole number of warps.
+template <typename T, int L, int DIM, int V> struct ZTile {
+  static constexpr int CB = int(sizeof(cvec<T>));
+  static constexpr int NB = DIM * (DIM + 1) / 2;
+  static constexpr int TPL = Plan<L, V>::TPL;
+  static constexpr int BUDGET = kclamp(kpow2floor(40960 / (L * NB * CB)), 1, 16);
+  static constexpr int G = (TPL % 32 == 0) ? 32 : (TPL % 16 == 0) ? 16 : (TPL % 8 == 0) ? 8
+                         : (TPL % 4 == 0) ? 4 : (TPL % 2 == 0) ? 2 : 1;  // gcd(TPL, 32)
+  static constexpr int MIN = DIM == 3 ? (G >= 16 ? 1 : 16 / G) : 32 / G;
+  static constexpr int NLP = BUDGET > MIN ? BUDGET : MIN;
+  static_assert((NB * NLP * TPL) % 32 == 0, "k_zpass needs whole warps");
 };
 
 template <typename K> inline cudaError_t set_smem(K kernel, size_t bytes) {
@@ -72,7 +90,14 @@ template <typename T, int L, int V> struct LaunchV {
     return cudaGetLastError();
   }
 
+  // The column kernels index rows with 32-bit offsets.
+  static bool rows_fit(const ColArgs& a) {
+    const long long lim = 0x7fffffffLL;
+    return (long long)L * a.in_row < lim && (long long)L * a.out_row < lim;
+  }
+
   static cudaError_t cols(int kind, const ColArgs& a, dim3 g, cudaStream_t st) {
+    if (!rows_fit(a)) return cudaErrorInvalidValue;
     switch (kind) {
       case COLK_PAD_INV: return col_kernel<+1, COL_PAD>(a, g, st);
       case COLK_PLAIN_INV: return col_kernel<+1, COL_PLAIN>(a, g, st);
@@ -99,6 +124,48 @@ template <typename T, int L, int V> struct LaunchV {
     return cudaErrorInvalidValue;
   }
 
+  // PERSIST: grid = resident CTAs, each walking chunks with two input
+  // buffers; otherwise one chunk per CTA and one buffer.
+  template <int DIM>
+  static cudaError_t zpass_kernel(const ZArgs& a, bool persist, cudaStream_t st) {
+    constexpr int NLP = ZTile<T, L, DIM, V>::NLP;
+    using Z = ZShape<T, L, NLP, DIM, V>;
+    auto k = k_zpass<T, L, NLP, DIM, V>;
+    const long long smem = Z::smem_bytes(a.nh, persist ? 2 : 1);
+    if (smem > 227 * 1024) return cudaErrorInvalidValue;
+    // The bulk copies need 16-byte aligned chunks of whole line pairs.
+    const long long lb = (long long)a.nh * DIM * Z::CB;
+    if ((reinterpret_cast<uintptr_t>(a.in) & 15) != 0 || (2 * lb) % 16 != 0 ||
+        (a.in_mem * Z::CB) % 16 != 0 || (a.nlines & 1) != 0)
+      return cudaErrorInvalidValue;
+    static const cudaError_t attr =
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    if (attr != cudaSuccess) return attr;
+    const long long chunks = (a.nlines + 2 * NLP - 1) / (2 * NLP);
+    const long long total = chunks * a.nmem;
+    long long cap = total;
+    if (persist) {
+      int dev = 0, sms = 0, per = 0;
+      cudaError_t ce = cudaGetDevice(&dev);
+      if (ce == cudaSuccess) ce = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      if (ce == cudaSuccess) ce = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, Z::NT, size_t(smem));
+      if (ce != cudaSuccess) return ce;
+      if (per < 1) return cudaErrorInvalidConfiguration;
+      cap = (long long)per * sms;
+    }
+    const long long grid = total < cap ? total : cap;
+    if (grid == 0) return cudaSuccess;
+    if (grid > 0x7fffffffLL) return cudaErrorInvalidValue;
+    k<<<unsigned(grid), Z::NT, size_t(smem), st>>>(a);
+    return cudaGetLastError();
+  }
+
+  static cudaError_t zpass(int dim, const ZArgs& a, bool persist, cudaStream_t st) {
+    if (dim == 2) return zpass_kernel<2>(a, persist, st);
+    if (dim == 3) return zpass_kernel<3>(a, persist, st);
+    return cudaErrorInvalidValue;
+  }
+
   template <int DIM, int NCM>
   static cudaError_t epi_kernel(const EpiArgs& a, dim3 g, cudaStream_t st) {
     constexpr int NB = DIM * (DIM + 1) / 2;
@@ -111,6 +178,9 @@ template <typename T, int L, int V> struct LaunchV {
   }
 
   static cudaError_t epi(int dim, const EpiArgs& a, dim3 g, cudaStream_t st) {
+    // 32-bit offsets: rows of B and one member's state.
+    const long long lim = 0x7fffffffLL;
+    if ((long long)L * a.B_row >= lim || (long long)dim * a.u_comp >= lim) return cudaErrorInvalidValue;
     if (dim == 2) return epi_kernel<2, TS::NCM2>(a, g, st);
     if (dim == 3) return epi_kernel<3, TS::NCM3>(a, g, st);
     return cudaErrorInvalidValue;
@@ -150,6 +220,10 @@ template <typename T, int L> struct Launch {
     const dim3 g(gx, gy, 1);
     return v ? LaunchV<T, L, 1>::rows(dim, a, g, st) : LaunchV<T, L, 0>::rows(dim, a, g, st);
   }
+  static cudaError_t zpass(int v, int dim, const ZArgs& a, cudaStream_t st) {
+    const bool persist = (v & 4) != 0;
+    return (v & 1) ? LaunchV<T, L, 1>::zpass(dim, a, persist, st) : LaunchV<T, L, 0>::zpass(dim, a, persist, st);
+  }
   static cudaError_t epilogue(int v, int dim, const EpiArgs& a, unsigned gx, unsigned gy,
                               cudaStream_t st) {
     const dim3 g(gx, gy, 1);
@@ -167,6 +241,7 @@ template <typename T, int L> struct Launch {
                                  {LaunchV<T, L, 0>::tiles(), LaunchV<T, L, 1>::tiles()},
                                  &cols,
                                  &rows_product,
+                                 &zpass,
                                  &epilogue,
                                  &c2r,
                                  &r2c};

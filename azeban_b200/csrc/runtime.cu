@@ -59,7 +59,7 @@ int tuned_variant(int precision, int L, int kind) {
   if (const char* env = std::getenv("AZ_PLAN_VARIANT")) {
     int v[3] = {0, 0, 0};
     if (std::sscanf(env, "%d,%d,%d", &v[0], &v[1], &v[2]) == 3 && kind >= 0 && kind < 6)
-      return v[kind % 3] ? 1 : 0;
+      return kind % 3 == 0 ? (v[0] & 1) : kind % 3 == 1 ? (v[1] & 7) : (v[2] & 1);
   }
   return precision == 1 ? 1 : 0;
 }
@@ -76,6 +76,14 @@ static az_status fail(az_status st, const std::string& msg) {
 
 static az_status cuda_fail(cudaError_t e, const char* what) {
   return fail(AZ_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// Status of a nonzero Ctrl::err word: bit 0 a non-finite value met by the CFL
+// reduction, bit 1 a bounded wait on a kernel's own bulk copy that ran out
+// (the kernel then returned early and its output is incomplete).
+static az_status ctrl_error(int err) {
+  if (err & 2) return fail(AZ_ERR_CUDA, "a bulk-copy wait inside a transform pass ran out; the pass is incomplete");
+  return fail(AZ_ERR_NONFINITE, "non-finite value in the CFL reduction");
 }
 
 #define AZB_CUDA(call)                                   \
@@ -303,6 +311,29 @@ size_t az_euler_workspace_size(az_euler e) { return e ? e->work_bytes : 0; }
 
 namespace azb {
 
+// The contiguous-axis product pass over every member.  Bits of the tuned
+// variant: 0 the radix plan, 1 the bulk-copy kernel (k_zpass) instead of
+// k_rows_product, 2 the persistent launch of k_zpass.
+static cudaError_t product_pass(az_euler e, int dim, const RowArgs& r, cudaStream_t st) {
+  const KernelSet* ks = e->ks;
+  if (e->v_rows & 2) {
+    ZArgs z{};
+    z.in = r.in;
+    z.out = r.out;
+    z.tw = r.tw;
+    z.nlines = r.nlines;
+    z.nh = r.nh;
+    z.nmem = e->batch;
+    z.in_mem = r.in_mem;
+    z.out_mem = r.out_mem;
+    z.norm = r.norm;
+    z.ctrl = r.ctrl;
+    return ks->zpass(e->v_rows & 5, dim, z, st);
+  }
+  const int nlp = dim == 3 ? ks->tiles[e->v_rows & 1].nlp3 : ks->tiles[e->v_rows & 1].nlp2;
+  return ks->rows_product(e->v_rows & 1, dim, r, unsigned(cdiv(r.nlines, 2 * nlp)), unsigned(e->batch), st);
+}
+
 // One right-hand side of every member: out <- stage(mode, u, u0, RHS(u)).
 // first_stage: compute dt = min(C/(N u_max), max_dt) after the product pass.
 static az_status rhs(az_euler e, const void* u, const void* u0, void* out, int mode, bool first_stage,
@@ -370,7 +401,7 @@ static az_status rhs(az_euler e, const void* u, const void* u0, void* out, int m
     r.ctrl = e->ctrl;
     {
       ProfScope ps(P_PRODUCT, double(B) * 9 * (M * M * Nh) * e->csize, st, e->prof);
-      ce = ks->rows_product(e->v_rows, 3, r, unsigned(cdiv(r.nlines, 2 * ks->tiles[e->v_rows].nlp3)), B, st);
+      ce = product_pass(e, 3, r, st);
     }
     if (ce != cudaSuccess) return cuda_fail(ce, "rhs pass 3");
   } else {
@@ -410,7 +441,7 @@ static az_status rhs(az_euler e, const void* u, const void* u0, void* out, int m
     r.ctrl = e->ctrl;
     {
       ProfScope ps(P_PRODUCT, double(B) * 5 * (M * Nh) * e->csize, st, e->prof);
-      ce = ks->rows_product(e->v_rows, 2, r, unsigned(cdiv(r.nlines, 2 * ks->tiles[e->v_rows].nlp2)), B, st);
+      ce = product_pass(e, 2, r, st);
     }
     if (ce != cudaSuccess) return cuda_fail(ce, "rhs pass 2 (2-D)");
   }
@@ -527,12 +558,13 @@ az_status az_euler_dt(az_euler e, double C, void* stream, double* out) {
     out[b] = C / ((double)e->N * u_max_);
   }
   for (int b = 0; b < e->batch; ++b)
-    if (h[b].err) return fail(AZ_ERR_NONFINITE, "non-finite value in the CFL reduction");
+    if (h[b].err) return ctrl_error(h[b].err);
   return AZ_OK;
 }
 
 az_status az_tune_set(int precision, int L, int kind, int variant) {
-  if ((precision != 0 && precision != 1) || kind < 0 || kind > 5 || (variant != 0 && variant != 1))
+  const int vmax = kind % 3 == 1 ? 7 : 1;
+  if ((precision != 0 && precision != 1) || kind < 0 || kind > 5 || variant < 0 || variant > vmax)
     return fail(AZ_ERR_INVALID, "az_tune_set: bad argument");
   if (!kernel_set(precision, L)) return fail(AZ_ERR_UNSUPPORTED, "az_tune_set: no compiled length");
   std::lock_guard<std::mutex> lock(g_tune_mutex);
@@ -635,7 +667,7 @@ az_status az_rk3_integrate(az_rk3 r, double t, double max_dt, double C, void* u_
   AZB_CUDA(cudaStreamSynchronize(st));
   for (int b = 0; b < e->batch; ++b) {
     if (dt_out) dt_out[b] = h[b].dt;
-    if (h[b].err) return fail(AZ_ERR_NONFINITE, "non-finite value in the CFL reduction");
+    if (h[b].err) return ctrl_error(h[b].err);
   }
   return AZ_OK;
 }
@@ -793,7 +825,7 @@ az_status az_sim_simulate_until(az_sim s, double t, void* stream) {
     double min_left = INFINITY;
     bool any = false;
     for (int b = 0; b < e->batch; ++b) {
-      if (s->host[b].err) return fail(AZ_ERR_NONFINITE, "non-finite value in the CFL reduction");
+      if (s->host[b].err) return ctrl_error(s->host[b].err);
       if (s->host[b].time < t) {
         any = true;
         const double dt = s->host[b].dt > 0 ? s->host[b].dt : 0.0;
@@ -963,7 +995,7 @@ az_status az_group_simulate_until(az_group g, double t, void* stream) {
     for (az_sim s : g->sims) {
       az_euler e = s->ts->eq;
       for (int b = 0; b < e->batch; ++b) {
-        if (s->host[b].err) return fail(AZ_ERR_NONFINITE, "non-finite value in the CFL reduction");
+        if (s->host[b].err) return ctrl_error(s->host[b].err);
         if (s->host[b].time < t) {
           any = true;
           const double dt = s->host[b].dt;
@@ -1179,7 +1211,7 @@ az_status az_fft_forward(az_fft f, void* stream) {
   r.nlines = lines;
   r.in_line = f->shape[last];
   r.out_line = f->nh;
-  const int v = tuned_variant(f->prec, int(f->shape[last]), 1);
+  const int v = tuned_variant(f->prec, int(f->shape[last]), 1) & 1;  // plan bit only
   cudaError_t ce = f->ks[last]->r2c(v, r, unsigned(cdiv(lines, 2 * f->ks[last]->tiles[v].nlpr)), st);
   if (ce != cudaSuccess) return cuda_fail(ce, "fft r2c pass");
   for (int ax = last - 1; ax >= f->dim - f->nt; --ax) {
@@ -1209,7 +1241,7 @@ az_status az_fft_backward(az_fft f, void* stream) {
   r.nlines = lines;
   r.in_line = f->nh;
   r.out_line = f->shape[last];
-  const int v = tuned_variant(f->prec, int(f->shape[last]), 1);
+  const int v = tuned_variant(f->prec, int(f->shape[last]), 1) & 1;  // plan bit only
   cudaError_t ce = f->ks[last]->c2r(v, r, unsigned(cdiv(lines, 2 * f->ks[last]->tiles[v].nlpr)), st);
   if (ce != cudaSuccess) return cuda_fail(ce, "fft c2r pass");
   return AZ_OK;

@@ -1,0 +1,330 @@
+// Contiguous-axis pass of the right-hand side, fed by TMA bulk copies.
+//
+// The work is the same as k_rows_product (c2r of the velocity lines, the CFL
+// maximum, B = u (x) u in the reference's component order, r2c of the
+// products, bins [0, nh) kept), but the input of a chunk of 2 NLP lines is one
+// contiguous run of global memory, so a single elected thread moves it into
+// shared memory with one cp.async.bulk, completing on an mbarrier: no thread
+// issues a global load.  A CTA walks chunks with a stride of gridDim.x; with
+// a grid smaller than the chunk count (the persistent launch) it keeps two
+// input buffers, and chunk t + gridDim.x is in flight while chunk t is
+// transformed.  Every mbarrier wait is bounded; a wait that runs out sets
+// bit 1 of the member's error word and the CTA leaves after draining its own
+// copies.
+//
+// Reference: the inverse transform, max_norm and computeB of
+// IncompressibleEuler::dudt (include/azeban/equations/incompressible_euler.hpp
+// :103-120, :168-228) and the forward transform that follows
+// (src/azeban/cuda/operations/cufft.cpp:133-149).
+#pragma once
+
+#include "euler_kernels.cuh"
+
+namespace azb {
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0u;
+}
+// Bounded wait on one phase of an mbarrier; false if it never completed.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
+  constexpr int kLimit = 1 << 22;
+  for (int i = 0; i < kLimit; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+// Orders this thread's earlier generic-proxy accesses of shared memory before
+// later async-proxy (bulk copy) accesses.
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+// One bulk copy global -> shared of `bytes` (a multiple of 16, both addresses
+// 16-byte aligned), completing as transaction bytes on `bar`.
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes,
+                                          unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// threadIdx.x read afresh at each use: keeps the compiler from hoisting the
+// per-thread index arithmetic of every transform stage out of the chunk loop,
+// which would hold it in registers across the whole loop body.
+__device__ __forceinline__ int opaque_tid() {
+  int t;
+  asm volatile("mov.u32 %0, %%tid.x;\n" : "=r"(t));
+  return t;
+}
+
+// Largest finite value: |x| <= kFiniteMax is false exactly for inf and NaN.
+template <typename T> constexpr T kFiniteMax = sizeof(T) == 4 ? T(3.40282346638528859811704183484516925e38)
+                                                               : T(1.79769313486231570814527423731704357e308);
+
+struct ZArgs {
+  const void* in;   // lines of nh x DIM complex, component innermost, contiguous
+  void* out;        // lines of nh x NB complex, component innermost
+  const void* tw;
+  long long nlines;  // lines per member (even)
+  int nh;            // spectral bins per line
+  int nmem;          // members
+  long long in_mem, out_mem;  // member strides (elements)
+  double norm;       // 1 / (N^{d/2} M^{d/2})
+  Ctrl* ctrl;
+};
+
+// Shared-memory layout of one CTA (bytes), shared by the kernel and its
+// launcher: two mbarriers, the twiddle table, the work area [L][SROW] and one
+// or two input buffers of one chunk each.  Work columns [0, NFWD) hold the
+// product transforms, columns [NFWD, NFWD + NINV) the velocity transforms, so
+// the products are written without overwriting their inputs.
+template <typename T, int L, int NLP, int DIM, int V> struct ZShape {
+  static constexpr int CB = int(sizeof(cvec<T>));
+  static constexpr int NB = DIM * (DIM + 1) / 2;
+  static constexpr int NINV = DIM * NLP;
+  static constexpr int NFWD = NB * NLP;
+  static constexpr int SROW = NFWD + NINV + 1;
+  static constexpr int TPL = Plan<L, V>::TPL;
+  static constexpr int NT = NFWD * TPL;
+  static constexpr int OFF_TW = 16;
+  static constexpr int OFF_WORK = OFF_TW + L * CB;
+  static constexpr int OFF_IN = OFF_WORK + ((L * SROW * CB + 15) / 16) * 16;
+  // complex elements of one chunk's input
+  static __host__ __device__ long long chunk_elems(int nh) { return 2LL * NLP * nh * DIM; }
+  static __host__ __device__ long long smem_bytes(int nh, int nbuf) {
+    return OFF_IN + nbuf * chunk_elems(nh) * CB;
+  }
+};
+
+template <typename T, int L, int NLP, int DIM, int V>
+__global__ void __launch_bounds__(ZShape<T, L, NLP, DIM, V>::NT) k_zpass(ZArgs a) {
+  using C = cvec<T>;
+  using P = Plan<L, V>;
+  using Z = ZShape<T, L, NLP, DIM, V>;
+  constexpr int NB = Z::NB;
+  constexpr int NINV = Z::NINV;
+  constexpr int NFWD = Z::NFWD;
+  constexpr int SROW = Z::SROW;
+  constexpr int TPL = Z::TPL;
+  constexpr int NT = Z::NT;
+  extern __shared__ __align__(16) unsigned char az_smem[];
+  unsigned long long* bar = reinterpret_cast<unsigned long long*>(az_smem);
+  C* tw = reinterpret_cast<C*>(az_smem + Z::OFF_TW);
+  C* sm = reinterpret_cast<C*>(az_smem + Z::OFF_WORK);
+  C* inb = reinterpret_cast<C*>(az_smem + Z::OFF_IN);
+  const int nh = a.nh;
+  const int in_line = nh * DIM;
+  const int out_line = nh * NB;
+  const int cel = 2 * NLP * in_line;
+  const long long chunks = (a.nlines + 2 * NLP - 1) / (2 * NLP);
+  const long long total = chunks * a.nmem;
+  const C* gin = reinterpret_cast<const C*>(a.in);
+
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_fence_init();
+  }
+  load_twiddles<C, L>(tw, reinterpret_cast<const C*>(a.tw));
+  __syncthreads();
+
+  auto skipped = [&](long long t) { return a.ctrl[t / chunks].skip != 0; };
+  // Elected thread: start the copy of chunk t into input buffer b.
+  auto issue = [&](long long t, int b) {
+    const long long member = t / chunks;
+    const long long line0 = (t % chunks) * 2 * NLP;
+    const long long nl = a.nlines - line0 < 2 * NLP ? a.nlines - line0 : 2 * NLP;
+    const unsigned bytes = unsigned(nl * in_line * Z::CB);
+    fence_proxy_async_smem();
+    mbar_expect_tx(&bar[b], bytes);
+    bulk_load(inb + b * cel, gin + member * a.in_mem + line0 * in_line, bytes, &bar[b]);
+  };
+
+  unsigned phase = 0u;  // bit b: parity of the next completion of buffer b
+  long long t = blockIdx.x;
+  if (threadIdx.x == 0 && t < total && !skipped(t)) issue(t, 0);
+  long long cur_member = -1;
+  T vmax = T(0);
+  bool bad = false;
+  // Per-warp flush of the CFL maximum of the member this CTA just left.
+  auto flush = [&](long long member) {
+    if (member < 0) return;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) vmax = fmax(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+    const unsigned anybad = __any_sync(0xffffffffu, bad);
+    if ((threadIdx.x & 31) == 0) {
+      atomic_max_abs<T>(a.ctrl + member, vmax);
+      if (anybad) atomicOr(&a.ctrl[member].err, 1);
+    }
+    vmax = T(0);
+    bad = false;
+  };
+
+  for (int k = 0; t < total; t += gridDim.x, ++k) {
+    const int b = k & 1;
+    const long long tn = t + gridDim.x;
+    const bool next_issued = tn < total && !skipped(tn);
+    // Buffer b ^ 1 was last read before the barrier that closed the previous
+    // chunk, so it is free.
+    if (threadIdx.x == 0 && next_issued) issue(tn, b ^ 1);
+    const long long member = t / chunks;
+    if (member != cur_member) {
+      flush(cur_member);
+      cur_member = member;
+    }
+    if (skipped(t)) continue;
+    const bool ok = mbar_wait_bounded(&bar[b], (phase >> b) & 1u);
+    phase ^= 1u << b;
+    if (__syncthreads_or(!ok)) {
+      if (threadIdx.x == 0) atomicOr(&a.ctrl[member].err, 2);
+      if (next_issued) mbar_wait_bounded(&bar[b ^ 1], (phase >> (b ^ 1)) & 1u);
+      return;
+    }
+    const long long line0 = (t % chunks) * 2 * NLP;
+    const C* cin = inb + b * cel;
+    const int tid = opaque_tid();
+    // Line pairs of this chunk that exist (nlines is even, so a pair is whole).
+    const int npairs = int((a.nlines - line0) / 2 < NLP ? (a.nlines - line0) / 2 : NLP);
+
+    // 1. Hermitian extension into the velocity columns: column (pair p, slot
+    //    q) holds signal 2q + i * signal 2q+1, signal s = component s % DIM of
+    //    line s / DIM of the pair.  Bin k < nh gives rows k and L - k; rows
+    //    [nh, L - nh] are zero.  The imaginary parts of bin 0 and bin L/2 are
+    //    dropped, as a c2r does.
+    for (int idx = tid; idx < NLP * nh; idx += NT) {
+      const int p = idx / nh;
+      const int kb = idx - p * nh;
+      C sg[2 * DIM];
+      const C* src = cin + (2 * p) * in_line + kb * DIM;
+#pragma unroll
+      for (int s = 0; s < 2 * DIM; ++s)
+        sg[s] = p < npairs ? src[(s / DIM) * in_line + s % DIM] : cmk<C>(T(0), T(0));
+      const bool edge = kb == 0 || 2 * kb == L;
+      if (edge) {
+#pragma unroll
+        for (int s = 0; s < 2 * DIM; ++s) sg[s].y = T(0);
+      }
+      C* row = sm + kb * SROW + NFWD + p * DIM;
+      C* mrow = sm + (L - kb) * SROW + NFWD + p * DIM;
+#pragma unroll
+      for (int q = 0; q < DIM; ++q) {
+        const C x = sg[2 * q], y = sg[2 * q + 1];
+        row[q] = cmk<C>(x.x - y.y, x.y + y.x);
+        if (!edge) mrow[q] = cmk<C>(x.x + y.y, y.x - x.y);
+      }
+    }
+    for (int idx = tid; idx < (L - 2 * nh + 1) * NINV; idx += NT) {
+      const int r = idx / NINV;
+      const int c = idx - r * NINV;
+      sm[(nh + r) * SROW + NFWD + c] = cmk<C>(T(0), T(0));
+    }
+    __syncthreads();
+
+    // 2. Inverse transforms of the velocity columns, in place.
+    {
+      const bool active = tid < NINV * TPL;
+      const int col = NFWD + (active ? tid % NINV : 0);
+      const int tl = active ? tid / NINV : 0;
+      fft_columns<C, +1, L, SROW, true, P>(
+          sm, tw, col, tl, [&](int m) { return sm[m * SROW + col]; },
+          [&](int m, C v) { sm[m * SROW + col] = v; }, active);
+    }
+    __syncthreads();
+
+    // 3. CFL maximum and products B = u (x) u in the reference's component
+    //    order (product c of line a in the real part, of line b in the
+    //    imaginary part), written to the product columns.
+    const T norm = T(a.norm);
+#pragma unroll
+    for (int p = 0; p < NLP; ++p) {
+#pragma unroll
+      for (int it = 0; it < (L + NT - 1) / NT; ++it) {
+        const int m = tid + it * NT;
+        if (L % NT == 0 || m < L) {
+          const C* v = sm + m * SROW + NFWD + p * DIM;
+          T u[2 * DIM];
+#pragma unroll
+          for (int q = 0; q < DIM; ++q) {
+            const C z = v[q];
+            u[2 * q] = z.x;
+            u[2 * q + 1] = z.y;
+          }
+#pragma unroll
+          for (int s = 0; s < 2 * DIM; ++s) {
+            const T av = fabs(u[s]);
+            bad |= !(av <= kFiniteMax<T>);
+            vmax = fmax(vmax, av);
+            u[s] *= norm;
+          }
+          C* w = sm + m * SROW + p * NB;
+          if constexpr (DIM == 2) {
+            w[0] = cmk<C>(u[0] * u[0], u[2] * u[2]);
+            w[1] = cmk<C>(u[0] * u[1], u[2] * u[3]);
+            w[2] = cmk<C>(u[1] * u[1], u[3] * u[3]);
+          } else {
+            w[0] = cmk<C>(u[0] * u[0], u[3] * u[3]);
+            w[1] = cmk<C>(u[1] * u[0], u[4] * u[3]);
+            w[2] = cmk<C>(u[1] * u[1], u[4] * u[4]);
+            w[3] = cmk<C>(u[2] * u[0], u[5] * u[3]);
+            w[4] = cmk<C>(u[2] * u[1], u[5] * u[4]);
+            w[5] = cmk<C>(u[2] * u[2], u[5] * u[5]);
+          }
+        }
+      }
+    }
+    __syncthreads();
+
+    // 4. Forward transforms of the NFWD product columns.
+    {
+      const int col = tid % NFWD;
+      const int tl = tid / NFWD;
+      fft_columns<C, -1, L, SROW, true, P>(
+          sm, tw, col, tl, [&](int m) { return sm[m * SROW + col]; },
+          [&](int m, C v) { sm[m * SROW + col] = v; });
+    }
+    __syncthreads();
+
+    // 5. Separate the two real spectra and write bins [0, nh): one thread per
+    //    (pair, bin) stores the NB components of that bin of both lines, so a
+    //    warp stores one contiguous run of each line.
+    C* out = reinterpret_cast<C*>(a.out) + member * a.out_mem + line0 * out_line;
+    for (int idx = tid; idx < npairs * nh; idx += NT) {
+      const int p = idx / nh;
+      const int kb = idx - p * nh;
+      const C* fk = sm + kb * SROW + p * NB;
+      const C* fm = sm + (kb == 0 ? 0 : L - kb) * SROW + p * NB;
+      C* oa = out + (2 * p) * out_line + kb * NB;
+      C* ob = oa + out_line;
+#pragma unroll
+      for (int c = 0; c < NB; ++c) {
+        const C x = fk[c], y = fm[c];
+        oa[c] = cmk<C>(T(0.5) * (x.x + y.x), T(0.5) * (x.y - y.y));
+        ob[c] = cmk<C>(T(0.5) * (x.y + y.y), T(-0.5) * (x.x - y.x));
+      }
+    }
+    // The work area and input buffer b are reused by the next chunk.
+    __syncthreads();
+  }
+  flush(cur_member);
+}
+
+}  // namespace azb

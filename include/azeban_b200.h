@@ -196,11 +196,14 @@ size_t az_fft_work_area_size(az_fft fft);
 /* ---- tuning table (no reference counterpart; the reference's nearest is
  *      optimal_fft_size reading a benchmark file, src/azeban/operations/fft.cpp:63-108) */
 
-/* Plan variant (0: at most 24 elements per thread; 1: wide, fewer shared-
- * memory exchanges) used for transform length L of a precision by one pass
+/* Kernel variant used for transform length L of a precision by one pass
  * kind: 0 column passes, 1 contiguous-axis passes, 2 epilogue pass of 3-D
- * solves (and of FFT<Dim>), 3-5 the same of 2-D solves.  Applies to solves
- * and FFTs created afterwards. */
+ * solves (and of FFT<Dim>), 3-5 the same of 2-D solves.  Bit 0 picks the
+ * radix plan (0: at most 24 elements per thread; 1: wide, fewer shared-memory
+ * exchanges).  Contiguous-axis passes of solves (kinds 1, 4) also take bit 1,
+ * the bulk-copy kernel, and bit 2, its persistent launch (variants 0-7; plain
+ * FFT<Dim> row transforms use bit 0 only).  Other kinds: variants 0-1.
+ * Applies to solves and FFTs created afterwards. */
 az_status az_tune_set(int precision, int L, int kind, int variant);
 az_status az_tune_get(int precision, int L, int kind, int* variant);
 

@@ -1,0 +1,95 @@
+"""Parity of every kernel variant of the right-hand side with the CPU oracle.
+
+The passes have several kernels: bit 0 of a variant picks the radix plan
+(0 std, 1 wide); for the contiguous-axis pass bit 1 picks the bulk-copy
+kernel and bit 2 its persistent launch.  The tuning table picks one per
+(precision, length, kind); these tests pin each one against the oracle, so a
+table entry can never select a kernel whose results differ.  Tolerances as in
+test_gpu_euler.py.
+"""
+
+import ctypes as ct
+
+import numpy as np
+import pytest
+import torch
+
+import azeban_b200 as az
+from azeban_b200 import _lib
+from oracle import euler_oracle as ora
+from tests.gpu_helpers import VISC_CFGS, random_field_hat, rel_l2, to_dev, to_host
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"f64": 1e-12, "f32": 1e-5}
+
+
+class _Variants:
+    """Sets the tuning table entries of one (precision, length) and restores
+    the previous ones on exit."""
+
+    def __init__(self, prec, L, dim, cols, rows, epi):
+        self.p = 0 if prec == "f64" else 1
+        self.L = L
+        kb = 3 if dim == 2 else 0
+        self.want = {kb + 0: cols, kb + 1: rows, kb + 2: epi}
+
+    def __enter__(self):
+        self.saved = {}
+        for kind, v in self.want.items():
+            old = ct.c_int()
+            _lib.check(_lib.lib.az_tune_get(self.p, self.L, kind, ct.byref(old)))
+            self.saved[kind] = old.value
+            _lib.check(_lib.lib.az_tune_set(self.p, self.L, kind, v))
+        return self
+
+    def __exit__(self, *exc):
+        for kind, v in self.saved.items():
+            _lib.check(_lib.lib.az_tune_set(self.p, self.L, kind, v))
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("dim,N", [(2, 32), (2, 64), (2, 128), (3, 16), (3, 32)])
+@pytest.mark.parametrize("cols,rows,epi", [(0, 0, 0), (1, 1, 1), (0, 2, 0), (1, 3, 1), (0, 6, 0), (1, 7, 1)])
+def test_dudt_every_variant(prec, dim, N, cols, rows, epi):
+    og = ora.Grid(dim, N)
+    g = az.Grid(dim, N)
+    oeq = ora.IncompressibleEuler(og, ora.make_viscosity(VISC_CFGS["smooth"], og))
+    u_hat = random_field_hat(dim, N, seed=300 + 10 * dim + N)
+    ref = oeq.dudt(u_hat)
+    with _Variants(prec, g.N_phys_pad, dim, cols, rows, epi):
+        eq = az.IncompressibleEuler(g, az.make_viscosity(VISC_CFGS["smooth"], g), prec)
+        d_u = to_dev(u_hat, prec)
+        d_out = torch.empty_like(d_u)
+        eq.dudt(d_out, d_u, 0.0, 0.0, 0.2)
+        got = to_host(d_out)
+        dt = eq.dt(0.2)
+    assert rel_l2(got, ref) <= TOL[prec]
+    rel_dt = 1e-13 if prec == "f64" else 1e-6
+    assert abs(dt - oeq.dt(0.2)) <= rel_dt * oeq.dt(0.2)
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("dim,N,B", [(2, 32, 7), (3, 16, 3)])
+@pytest.mark.parametrize("rows", [2, 6])
+def test_bulk_copy_kernel_batch_members_match_single(prec, dim, N, B, rows):
+    """With the bulk-copy kernel (and its persistent launch, where a CTA walks
+    chunks of several members), each member of a batch equals the same solve
+    alone, bit for bit, over a short simulate_until.  Members have different
+    amplitudes, so they finish at different steps and the skip flags are
+    exercised."""
+    g = az.Grid(dim, N)
+    v = az.make_viscosity(VISC_CFGS["smooth"], g)
+    fields = [random_field_hat(dim, N, seed=900 + b) * (1.0 + 0.5 * b) for b in range(B)]
+    with _Variants(prec, g.N_phys_pad, dim, 0, rows, 0):
+        eqB = az.IncompressibleEuler(g, v, prec, batch=B)
+        simB = az.Simulation(g, 0.2, az.SSP_RK3(eqB), to_dev(np.stack(fields), prec))
+        simB.simulate_until(0.02)
+        outB = to_host(simB.u())
+        _, nB, _ = simB.state()
+        for b in range(B):
+            eq1 = az.IncompressibleEuler(g, v, prec)
+            sim1 = az.Simulation(g, 0.2, az.SSP_RK3(eq1), to_dev(fields[b], prec))
+            sim1.simulate_until(0.02)
+            assert sim1.state()[1][0] == nB[b]
+            np.testing.assert_array_equal(to_host(sim1.u()), outB[b])
