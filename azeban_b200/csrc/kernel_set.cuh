@@ -30,8 +30,7 @@ struct KernelSet {
   TileShape tiles[2];  // per plan variant (bit 0 of a variant number)
   cudaError_t (*cols)(int v, int kind, const ColArgs&, unsigned gx, unsigned gy, unsigned gz, cudaStream_t);
   cudaError_t (*rows_product)(int v, int dim, const RowArgs&, unsigned gx, unsigned gy, cudaStream_t);
-  // Bulk-copy form of the product pass: plan variant v & 1; v & 4 selects the
-  // persistent, double-buffered launch.
+  // Bulk-copy form of the product pass (plan variant v & 1).
   cudaError_t (*zpass)(int v, int dim, const ZArgs&, cudaStream_t);
   cudaError_t (*epilogue)(int v, int dim, const EpiArgs&, unsigned gx, unsigned gy, cudaStream_t);
   cudaError_t (*c2r)(int v, const RealRowArgs&, unsigned gx, cudaStream_t);
@@ -55,13 +54,13 @@ template <typename T, int L, int V> struct Tiles {
   static constexpr int NLPR = kclamp(kpow2floor(49152 / (L * CB)), 1, 64);
 };
 
-// Line pairs per chunk of k_zpass: about 40 KB of work area, raised until the
+// Line pairs per chunk of k_zpass: about 80 KB of work area, raised until the
 // CTA's thread count is a whole number of warps.
 template <typename T, int L, int DIM, int V> struct ZTile {
   static constexpr int CB = int(sizeof(cvec<T>));
   static constexpr int NB = DIM * (DIM + 1) / 2;
   static constexpr int TPL = Plan<L, V>::TPL;
-  static constexpr int BUDGET = kclamp(kpow2floor(40960 / (L * NB * CB)), 1, 16);
+  static constexpr int BUDGET = kclamp(kpow2floor(81920 / (L * NB * CB)), 1, 16);
   static constexpr int G = (TPL % 32 == 0) ? 32 : (TPL % 16 == 0) ? 16 : (TPL % 8 == 0) ? 8
                          : (TPL % 4 == 0) ? 4 : (TPL % 2 == 0) ? 2 : 1;  // gcd(TPL, 32)
   static constexpr int MIN = DIM == 3 ? (G >= 16 ? 1 : 16 / G) : 32 / G;
@@ -124,16 +123,14 @@ template <typename T, int L, int V> struct LaunchV {
     return cudaErrorInvalidValue;
   }
 
-  // PERSIST: grid = resident CTAs, each walking chunks with two input
-  // buffers; otherwise one chunk per CTA and one buffer.
   template <int DIM>
-  static cudaError_t zpass_kernel(const ZArgs& a, bool persist, cudaStream_t st) {
+  static cudaError_t zpass(const ZArgs& a, cudaStream_t st) {
     constexpr int NLP = ZTile<T, L, DIM, V>::NLP;
     using Z = ZShape<T, L, NLP, DIM, V>;
     auto k = k_zpass<T, L, NLP, DIM, V>;
-    const long long smem = Z::smem_bytes(a.nh, persist ? 2 : 1);
+    const long long smem = Z::smem_bytes(a.nh);
     if (smem > 227 * 1024) return cudaErrorInvalidValue;
-    // The bulk copies need 16-byte aligned chunks of whole line pairs.
+    // The bulk copy needs a 16-byte aligned chunk of whole line pairs.
     const long long lb = (long long)a.nh * DIM * Z::CB;
     if ((reinterpret_cast<uintptr_t>(a.in) & 15) != 0 || (2 * lb) % 16 != 0 ||
         (a.in_mem * Z::CB) % 16 != 0 || (a.nlines & 1) != 0)
@@ -142,27 +139,15 @@ template <typename T, int L, int V> struct LaunchV {
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
     if (attr != cudaSuccess) return attr;
     const long long chunks = (a.nlines + 2 * NLP - 1) / (2 * NLP);
-    const long long total = chunks * a.nmem;
-    long long cap = total;
-    if (persist) {
-      int dev = 0, sms = 0, per = 0;
-      cudaError_t ce = cudaGetDevice(&dev);
-      if (ce == cudaSuccess) ce = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-      if (ce == cudaSuccess) ce = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, Z::NT, size_t(smem));
-      if (ce != cudaSuccess) return ce;
-      if (per < 1) return cudaErrorInvalidConfiguration;
-      cap = (long long)per * sms;
-    }
-    const long long grid = total < cap ? total : cap;
-    if (grid == 0) return cudaSuccess;
-    if (grid > 0x7fffffffLL) return cudaErrorInvalidValue;
-    k<<<unsigned(grid), Z::NT, size_t(smem), st>>>(a);
+    if (chunks == 0 || a.nmem == 0) return cudaSuccess;
+    if (chunks > 0x7fffffffLL || a.nmem > 65535) return cudaErrorInvalidValue;
+    k<<<dim3(unsigned(chunks), unsigned(a.nmem)), Z::NT, size_t(smem), st>>>(a);
     return cudaGetLastError();
   }
 
-  static cudaError_t zpass(int dim, const ZArgs& a, bool persist, cudaStream_t st) {
-    if (dim == 2) return zpass_kernel<2>(a, persist, st);
-    if (dim == 3) return zpass_kernel<3>(a, persist, st);
+  static cudaError_t zpass(int dim, const ZArgs& a, cudaStream_t st) {
+    if (dim == 2) return zpass<2>(a, st);
+    if (dim == 3) return zpass<3>(a, st);
     return cudaErrorInvalidValue;
   }
 
@@ -221,8 +206,7 @@ template <typename T, int L> struct Launch {
     return v ? LaunchV<T, L, 1>::rows(dim, a, g, st) : LaunchV<T, L, 0>::rows(dim, a, g, st);
   }
   static cudaError_t zpass(int v, int dim, const ZArgs& a, cudaStream_t st) {
-    const bool persist = (v & 4) != 0;
-    return (v & 1) ? LaunchV<T, L, 1>::zpass(dim, a, persist, st) : LaunchV<T, L, 0>::zpass(dim, a, persist, st);
+    return (v & 1) ? LaunchV<T, L, 1>::zpass(dim, a, st) : LaunchV<T, L, 0>::zpass(dim, a, st);
   }
   static cudaError_t epilogue(int v, int dim, const EpiArgs& a, unsigned gx, unsigned gy,
                               cudaStream_t st) {

@@ -59,7 +59,7 @@ int tuned_variant(int precision, int L, int kind) {
   if (const char* env = std::getenv("AZ_PLAN_VARIANT")) {
     int v[3] = {0, 0, 0};
     if (std::sscanf(env, "%d,%d,%d", &v[0], &v[1], &v[2]) == 3 && kind >= 0 && kind < 6)
-      return kind % 3 == 0 ? (v[0] & 1) : kind % 3 == 1 ? (v[1] & 7) : (v[2] & 1);
+      return kind % 3 == 1 ? (v[1] & 3) : (v[kind % 3] & 1);
   }
   return precision == 1 ? 1 : 0;
 }
@@ -313,7 +313,7 @@ namespace azb {
 
 // The contiguous-axis product pass over every member.  Bits of the tuned
 // variant: 0 the radix plan, 1 the bulk-copy kernel (k_zpass) instead of
-// k_rows_product, 2 the persistent launch of k_zpass.
+// k_rows_product.
 static cudaError_t product_pass(az_euler e, int dim, const RowArgs& r, cudaStream_t st) {
   const KernelSet* ks = e->ks;
   if (e->v_rows & 2) {
@@ -328,7 +328,7 @@ static cudaError_t product_pass(az_euler e, int dim, const RowArgs& r, cudaStrea
     z.out_mem = r.out_mem;
     z.norm = r.norm;
     z.ctrl = r.ctrl;
-    return ks->zpass(e->v_rows & 5, dim, z, st);
+    return ks->zpass(e->v_rows & 1, dim, z, st);
   }
   const int nlp = dim == 3 ? ks->tiles[e->v_rows & 1].nlp3 : ks->tiles[e->v_rows & 1].nlp2;
   return ks->rows_product(e->v_rows & 1, dim, r, unsigned(cdiv(r.nlines, 2 * nlp)), unsigned(e->batch), st);
@@ -563,7 +563,7 @@ az_status az_euler_dt(az_euler e, double C, void* stream, double* out) {
 }
 
 az_status az_tune_set(int precision, int L, int kind, int variant) {
-  const int vmax = kind % 3 == 1 ? 7 : 1;
+  const int vmax = kind % 3 == 1 ? 3 : 1;
   if ((precision != 0 && precision != 1) || kind < 0 || kind > 5 || variant < 0 || variant > vmax)
     return fail(AZ_ERR_INVALID, "az_tune_set: bad argument");
   if (!kernel_set(precision, L)) return fail(AZ_ERR_UNSUPPORTED, "az_tune_set: no compiled length");

@@ -1,16 +1,14 @@
-// Contiguous-axis pass of the right-hand side, fed by TMA bulk copies.
+// Contiguous-axis pass of the right-hand side, fed by a TMA bulk copy.
 //
 // The work is the same as k_rows_product (c2r of the velocity lines, the CFL
 // maximum, B = u (x) u in the reference's component order, r2c of the
-// products, bins [0, nh) kept), but the input of a chunk of 2 NLP lines is one
-// contiguous run of global memory, so a single elected thread moves it into
-// shared memory with one cp.async.bulk, completing on an mbarrier: no thread
-// issues a global load.  A CTA walks chunks with a stride of gridDim.x; with
-// a grid smaller than the chunk count (the persistent launch) it keeps two
-// input buffers, and chunk t + gridDim.x is in flight while chunk t is
-// transformed.  Every mbarrier wait is bounded; a wait that runs out sets
-// bit 1 of the member's error word and the CTA leaves after draining its own
-// copies.
+// products, bins [0, nh) kept), but the input of a CTA's chunk of 2 NLP lines
+// is one contiguous run of global memory, so a single elected thread moves it
+// into shared memory with one cp.async.bulk, completing on an mbarrier: no
+// thread issues a global load, and the phases that follow index shared memory
+// with plain row/column arithmetic instead of a Hermitian-extension gather.
+// The mbarrier wait is bounded; a wait that runs out sets bit 1 of the
+// member's error word and the CTA returns.
 //
 // Reference: the inverse transform, max_norm and computeB of
 // IncompressibleEuler::dudt (include/azeban/equations/incompressible_euler.hpp
@@ -51,11 +49,6 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsig
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
-// Orders this thread's earlier generic-proxy accesses of shared memory before
-// later async-proxy (bulk copy) accesses.
-__device__ __forceinline__ void fence_proxy_async_smem() {
-  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-}
 // One bulk copy global -> shared of `bytes` (a multiple of 16, both addresses
 // 16-byte aligned), completing as transaction bytes on `bar`.
 __device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes,
@@ -65,15 +58,6 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned b
           smem_u32(dst)),
       "l"(src), "r"(bytes), "r"(smem_u32(bar))
       : "memory");
-}
-
-// threadIdx.x read afresh at each use: keeps the compiler from hoisting the
-// per-thread index arithmetic of every transform stage out of the chunk loop,
-// which would hold it in registers across the whole loop body.
-__device__ __forceinline__ int opaque_tid() {
-  int t;
-  asm volatile("mov.u32 %0, %%tid.x;\n" : "=r"(t));
-  return t;
 }
 
 // Largest finite value: |x| <= kFiniteMax is false exactly for inf and NaN.
@@ -93,30 +77,35 @@ struct ZArgs {
 };
 
 // Shared-memory layout of one CTA (bytes), shared by the kernel and its
-// launcher: two mbarriers, the twiddle table, the work area [L][SROW] and one
-// or two input buffers of one chunk each.  Work columns [0, NFWD) hold the
-// product transforms, columns [NFWD, NFWD + NINV) the velocity transforms, so
-// the products are written without overwriting their inputs.
+// launcher: the mbarrier, the twiddle table, the work area [L][SROW] and the
+// chunk's input.  Work columns [0, NFWD) hold the
+// product transforms; the velocity transforms sit at the end of the same
+// rows, columns [VOFF, NFWD).  The product columns of pair p overlap only
+// velocity columns of pairs <= p, so a thread that owns a row and handles its
+// pairs in order writes the products in place, after reading what they cover.
 template <typename T, int L, int NLP, int DIM, int V> struct ZShape {
   static constexpr int CB = int(sizeof(cvec<T>));
   static constexpr int NB = DIM * (DIM + 1) / 2;
   static constexpr int NINV = DIM * NLP;
   static constexpr int NFWD = NB * NLP;
-  static constexpr int SROW = NFWD + NINV + 1;
+  static constexpr int VOFF = NFWD - NINV;
+  static constexpr int SROW = NFWD + 1;
   static constexpr int TPL = Plan<L, V>::TPL;
   static constexpr int NT = NFWD * TPL;
+  // FP32 std plans: ask for 16 resident warps per SM (a register cap the
+  // compiler meets without spills); wide and FP64 plans need their registers.
+  static constexpr int MINB = (V == 0 && CB == 8) ? (512 + NT - 1) / NT : 1;
   static constexpr int OFF_TW = 16;
   static constexpr int OFF_WORK = OFF_TW + L * CB;
   static constexpr int OFF_IN = OFF_WORK + ((L * SROW * CB + 15) / 16) * 16;
   // complex elements of one chunk's input
   static __host__ __device__ long long chunk_elems(int nh) { return 2LL * NLP * nh * DIM; }
-  static __host__ __device__ long long smem_bytes(int nh, int nbuf) {
-    return OFF_IN + nbuf * chunk_elems(nh) * CB;
-  }
+  static __host__ __device__ long long smem_bytes(int nh) { return OFF_IN + chunk_elems(nh) * CB; }
 };
 
 template <typename T, int L, int NLP, int DIM, int V>
-__global__ void __launch_bounds__(ZShape<T, L, NLP, DIM, V>::NT) k_zpass(ZArgs a) {
+__global__ void __launch_bounds__(ZShape<T, L, NLP, DIM, V>::NT, ZShape<T, L, NLP, DIM, V>::MINB)
+    k_zpass(ZArgs a) {
   using C = cvec<T>;
   using P = Plan<L, V>;
   using Z = ZShape<T, L, NLP, DIM, V>;
@@ -124,86 +113,43 @@ __global__ void __launch_bounds__(ZShape<T, L, NLP, DIM, V>::NT) k_zpass(ZArgs a
   constexpr int NINV = Z::NINV;
   constexpr int NFWD = Z::NFWD;
   constexpr int SROW = Z::SROW;
+  constexpr int VOFF = Z::VOFF;
   constexpr int TPL = Z::TPL;
   constexpr int NT = Z::NT;
   extern __shared__ __align__(16) unsigned char az_smem[];
   unsigned long long* bar = reinterpret_cast<unsigned long long*>(az_smem);
   C* tw = reinterpret_cast<C*>(az_smem + Z::OFF_TW);
   C* sm = reinterpret_cast<C*>(az_smem + Z::OFF_WORK);
-  C* inb = reinterpret_cast<C*>(az_smem + Z::OFF_IN);
+  const C* cin = reinterpret_cast<const C*>(az_smem + Z::OFF_IN);
+  const int member = blockIdx.y;
+  Ctrl* ctrl = a.ctrl + member;
+  if (ctrl->skip) return;
+  const int tid = threadIdx.x;
   const int nh = a.nh;
   const int in_line = nh * DIM;
   const int out_line = nh * NB;
-  const int cel = 2 * NLP * in_line;
-  const long long chunks = (a.nlines + 2 * NLP - 1) / (2 * NLP);
-  const long long total = chunks * a.nmem;
-  const C* gin = reinterpret_cast<const C*>(a.in);
+  const long long line0 = (long long)blockIdx.x * 2 * NLP;
+  // Line pairs of this chunk that exist (nlines is even, so a pair is whole).
+  const int npairs = int((a.nlines - line0) / 2 < NLP ? (a.nlines - line0) / 2 : NLP);
 
-  if (threadIdx.x == 0) {
+  // Elected thread: one bulk copy of the chunk's lines into shared memory.
+  if (tid == 0) {
     mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
     mbar_fence_init();
+    const unsigned bytes = unsigned(2 * npairs * in_line * Z::CB);
+    mbar_expect_tx(&bar[0], bytes);
+    bulk_load(az_smem + Z::OFF_IN,
+              reinterpret_cast<const C*>(a.in) + member * a.in_mem + line0 * in_line, bytes, &bar[0]);
   }
   load_twiddles<C, L>(tw, reinterpret_cast<const C*>(a.tw));
   __syncthreads();
-
-  auto skipped = [&](long long t) { return a.ctrl[t / chunks].skip != 0; };
-  // Elected thread: start the copy of chunk t into input buffer b.
-  auto issue = [&](long long t, int b) {
-    const long long member = t / chunks;
-    const long long line0 = (t % chunks) * 2 * NLP;
-    const long long nl = a.nlines - line0 < 2 * NLP ? a.nlines - line0 : 2 * NLP;
-    const unsigned bytes = unsigned(nl * in_line * Z::CB);
-    fence_proxy_async_smem();
-    mbar_expect_tx(&bar[b], bytes);
-    bulk_load(inb + b * cel, gin + member * a.in_mem + line0 * in_line, bytes, &bar[b]);
-  };
-
-  unsigned phase = 0u;  // bit b: parity of the next completion of buffer b
-  long long t = blockIdx.x;
-  if (threadIdx.x == 0 && t < total && !skipped(t)) issue(t, 0);
-  long long cur_member = -1;
+  const bool ok = mbar_wait_bounded(&bar[0], 0u);
+  if (__syncthreads_or(!ok)) {
+    if (tid == 0) atomicOr(&ctrl->err, 2);
+    return;
+  }
   T vmax = T(0);
   bool bad = false;
-  // Per-warp flush of the CFL maximum of the member this CTA just left.
-  auto flush = [&](long long member) {
-    if (member < 0) return;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) vmax = fmax(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
-    const unsigned anybad = __any_sync(0xffffffffu, bad);
-    if ((threadIdx.x & 31) == 0) {
-      atomic_max_abs<T>(a.ctrl + member, vmax);
-      if (anybad) atomicOr(&a.ctrl[member].err, 1);
-    }
-    vmax = T(0);
-    bad = false;
-  };
-
-  for (int k = 0; t < total; t += gridDim.x, ++k) {
-    const int b = k & 1;
-    const long long tn = t + gridDim.x;
-    const bool next_issued = tn < total && !skipped(tn);
-    // Buffer b ^ 1 was last read before the barrier that closed the previous
-    // chunk, so it is free.
-    if (threadIdx.x == 0 && next_issued) issue(tn, b ^ 1);
-    const long long member = t / chunks;
-    if (member != cur_member) {
-      flush(cur_member);
-      cur_member = member;
-    }
-    if (skipped(t)) continue;
-    const bool ok = mbar_wait_bounded(&bar[b], (phase >> b) & 1u);
-    phase ^= 1u << b;
-    if (__syncthreads_or(!ok)) {
-      if (threadIdx.x == 0) atomicOr(&a.ctrl[member].err, 2);
-      if (next_issued) mbar_wait_bounded(&bar[b ^ 1], (phase >> (b ^ 1)) & 1u);
-      return;
-    }
-    const long long line0 = (t % chunks) * 2 * NLP;
-    const C* cin = inb + b * cel;
-    const int tid = opaque_tid();
-    // Line pairs of this chunk that exist (nlines is even, so a pair is whole).
-    const int npairs = int((a.nlines - line0) / 2 < NLP ? (a.nlines - line0) / 2 : NLP);
 
     // 1. Hermitian extension into the velocity columns: column (pair p, slot
     //    q) holds signal 2q + i * signal 2q+1, signal s = component s % DIM of
@@ -223,8 +169,8 @@ __global__ void __launch_bounds__(ZShape<T, L, NLP, DIM, V>::NT) k_zpass(ZArgs a
 #pragma unroll
         for (int s = 0; s < 2 * DIM; ++s) sg[s].y = T(0);
       }
-      C* row = sm + kb * SROW + NFWD + p * DIM;
-      C* mrow = sm + (L - kb) * SROW + NFWD + p * DIM;
+      C* row = sm + kb * SROW + VOFF + p * DIM;
+      C* mrow = sm + (L - kb) * SROW + VOFF + p * DIM;
 #pragma unroll
       for (int q = 0; q < DIM; ++q) {
         const C x = sg[2 * q], y = sg[2 * q + 1];
@@ -235,14 +181,14 @@ __global__ void __launch_bounds__(ZShape<T, L, NLP, DIM, V>::NT) k_zpass(ZArgs a
     for (int idx = tid; idx < (L - 2 * nh + 1) * NINV; idx += NT) {
       const int r = idx / NINV;
       const int c = idx - r * NINV;
-      sm[(nh + r) * SROW + NFWD + c] = cmk<C>(T(0), T(0));
+      sm[(nh + r) * SROW + VOFF + c] = cmk<C>(T(0), T(0));
     }
     __syncthreads();
 
     // 2. Inverse transforms of the velocity columns, in place.
     {
       const bool active = tid < NINV * TPL;
-      const int col = NFWD + (active ? tid % NINV : 0);
+      const int col = VOFF + (active ? tid % NINV : 0);
       const int tl = active ? tid / NINV : 0;
       fft_columns<C, +1, L, SROW, true, P>(
           sm, tw, col, tl, [&](int m) { return sm[m * SROW + col]; },
@@ -252,15 +198,17 @@ __global__ void __launch_bounds__(ZShape<T, L, NLP, DIM, V>::NT) k_zpass(ZArgs a
 
     // 3. CFL maximum and products B = u (x) u in the reference's component
     //    order (product c of line a in the real part, of line b in the
-    //    imaginary part), written to the product columns.
+    //    imaginary part), in place: a thread owns rows and handles the pairs
+    //    of a row in order.
     const T norm = T(a.norm);
 #pragma unroll
-    for (int p = 0; p < NLP; ++p) {
+    for (int it = 0; it < (L + NT - 1) / NT; ++it) {
+      const int m = tid + it * NT;
+      if (L % NT != 0 && m >= L) break;
 #pragma unroll
-      for (int it = 0; it < (L + NT - 1) / NT; ++it) {
-        const int m = tid + it * NT;
-        if (L % NT == 0 || m < L) {
-          const C* v = sm + m * SROW + NFWD + p * DIM;
+      for (int p = 0; p < NLP; ++p) {
+        {
+          const C* v = sm + m * SROW + VOFF + p * DIM;
           T u[2 * DIM];
 #pragma unroll
           for (int q = 0; q < DIM; ++q) {
@@ -321,10 +269,26 @@ __global__ void __launch_bounds__(ZShape<T, L, NLP, DIM, V>::NT) k_zpass(ZArgs a
         ob[c] = cmk<C>(T(0.5) * (x.y + y.y), T(-0.5) * (x.x - y.x));
       }
     }
-    // The work area and input buffer b are reused by the next chunk.
-    __syncthreads();
+    // CFL reduction: warp, then block, then one atomic per CTA.
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) vmax = fmax(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+  const unsigned anybad = __any_sync(0xffffffffu, bad);
+  __shared__ T red[NT / 32];
+  __shared__ int redbad;
+  if (tid == 0) redbad = 0;
+  __syncthreads();
+  if ((tid & 31) == 0) {
+    red[tid >> 5] = vmax;
+    if (anybad) redbad = 1;
   }
-  flush(cur_member);
+  __syncthreads();
+  if (tid == 0) {
+    T m = T(0);
+#pragma unroll
+    for (int w = 0; w < NT / 32; ++w) m = fmax(m, red[w]);
+    atomic_max_abs<T>(ctrl, m);
+    if (redbad) atomicOr(&ctrl->err, 1);
+  }
 }
 
 }  // namespace azb

@@ -31,9 +31,9 @@ VISC = {"type": "Smooth Cutoff", "eps": 0.05}
 
 
 # Kernel variants: bit 0 picks the radix plan (0 std, 1 wide); for the
-# contiguous-axis pass bit 1 picks the bulk-copy kernel and bit 2 its
-# persistent launch.  The other kinds have plan variants only.
-RUNS = (0, 1, 2, 3, 6, 7)
+# contiguous-axis pass bit 1 picks the bulk-copy kernel.  The other kinds have
+# plan variants only.
+RUNS = (0, 1, 2, 3)
 
 
 def _kind_variant(kind0: int, run: int) -> int:

@@ -201,8 +201,8 @@ size_t az_fft_work_area_size(az_fft fft);
  * solves (and of FFT<Dim>), 3-5 the same of 2-D solves.  Bit 0 picks the
  * radix plan (0: at most 24 elements per thread; 1: wide, fewer shared-memory
  * exchanges).  Contiguous-axis passes of solves (kinds 1, 4) also take bit 1,
- * the bulk-copy kernel, and bit 2, its persistent launch (variants 0-7; plain
- * FFT<Dim> row transforms use bit 0 only).  Other kinds: variants 0-1.
+ * the bulk-copy kernel (variants 0-3; plain FFT<Dim> row transforms use bit 0
+ * only).  Other kinds: variants 0-1.
  * Applies to solves and FFTs created afterwards. */
 az_status az_tune_set(int precision, int L, int kind, int variant);
 az_status az_tune_get(int precision, int L, int kind, int* variant);
