@@ -332,18 +332,19 @@ struct Engine {
   // Runs every stage.  On entry v holds the first stage's inputs (rows given
   // by in_row<R0>); on exit v holds the last stage's outputs (rows given by
   // out_row<RL>).  Every thread of the CTA must call it (it contains
-  // barriers); threads with active == false compute but never write.  Each
-  // exchange starts with a barrier, so inputs may have come from sm.
+  // barriers); threads with active == false take part in the barriers only
+  // (no arithmetic, no shared-memory traffic).  Each exchange starts with a
+  // barrier, so inputs may have come from sm.
   template <int NS, int R, int... Rest>
   static __device__ __forceinline__ void run(C* sm, C (&v)[E], int col, int tl, const C* tw,
                                              bool active, Radices<R, Rest...>) {
-    compute<NS, R>(v, tl, tw);
+    if (active) compute<NS, R>(v, tl, tw);
     if constexpr (sizeof...(Rest) > 0) {
       __syncthreads();
       store_smem<NS, R>(sm, v, col, tl, active);
       __syncthreads();
       constexpr int RN = RadixInfo<Radices<Rest...>>::first;
-      load_smem<RN>(sm, v, col, tl);
+      if (active) load_smem<RN>(sm, v, col, tl);
       run<NS * R, Rest...>(sm, v, col, tl, tw, active, Radices<Rest...>{});
     }
   }
@@ -353,7 +354,8 @@ struct Engine {
 //   load(row) -> C     gives the first-stage input at `row`
 //   store(row, C)      receives output bin `row`
 // SYNC_STORE: put a barrier before the stores (needed when they go to sm).
-// Threads with active == false take part in the barriers only.
+// Threads with active == false take part in the barriers only: they neither
+// load, compute nor store.
 template <typename C, int S, int L, int SROW, bool SYNC_STORE, typename P = Plan<L>, typename Load,
           typename Store>
 __device__ __forceinline__ void fft_columns(C* sm, const C* tw, int col, int tl, Load&& load,
@@ -361,11 +363,13 @@ __device__ __forceinline__ void fft_columns(C* sm, const C* tw, int col, int tl,
   using Info = RadixInfo<typename P::R>;
   using Eng = Engine<C, S, L, P::E, SROW>;
   C v[P::E];
+  if (active) {
 #pragma unroll
-  for (int q = 0; q < P::E / Info::first; ++q) {
+    for (int q = 0; q < P::E / Info::first; ++q) {
 #pragma unroll
-    for (int r = 0; r < Info::first; ++r) {
-      v[q * Info::first + r] = load(Eng::template in_row<Info::first>(tl, q, r));
+      for (int r = 0; r < Info::first; ++r) {
+        v[q * Info::first + r] = load(Eng::template in_row<Info::first>(tl, q, r));
+      }
     }
   }
   Eng::template run<1>(sm, v, col, tl, tw, active, typename P::R{});

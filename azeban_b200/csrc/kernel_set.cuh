@@ -135,9 +135,17 @@ template <typename T, int L, int V> struct LaunchV {
     if ((reinterpret_cast<uintptr_t>(a.in) & 15) != 0 || (2 * lb) % 16 != 0 ||
         (a.in_mem * Z::CB) % 16 != 0 || (a.nlines & 1) != 0)
       return cudaErrorInvalidValue;
-    static const cudaError_t attr =
-        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-    if (attr != cudaSuccess) return attr;
+    // Raise the kernel's dynamic shared-memory limit to what this launch needs
+    // (the kernel also holds a little static shared memory).
+    static long long granted = 48 * 1024;
+    if (smem > granted) {
+      const cudaError_t ce = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+      if (ce != cudaSuccess) {
+        cudaGetLastError();
+        return ce;
+      }
+      granted = smem;
+    }
     const long long chunks = (a.nlines + 2 * NLP - 1) / (2 * NLP);
     if (chunks == 0 || a.nmem == 0) return cudaSuccess;
     if (chunks > 0x7fffffffLL || a.nmem > 65535) return cudaErrorInvalidValue;

@@ -251,24 +251,24 @@ __global__ void __launch_bounds__(ZShape<T, L, NLP, DIM, V>::NT, ZShape<T, L, NL
     }
     __syncthreads();
 
-    // 5. Separate the two real spectra and write bins [0, nh): one thread per
-    //    (pair, bin) stores the NB components of that bin of both lines, so a
-    //    warp stores one contiguous run of each line.
+    // 5. Separate the two real spectra and write bins [0, nh), component
+    //    fastest, so consecutive threads store consecutive elements of a line.
     C* out = reinterpret_cast<C*>(a.out) + member * a.out_mem + line0 * out_line;
-    for (int idx = tid; idx < npairs * nh; idx += NT) {
-      const int p = idx / nh;
-      const int kb = idx - p * nh;
-      const C* fk = sm + kb * SROW + p * NB;
-      const C* fm = sm + (kb == 0 ? 0 : L - kb) * SROW + p * NB;
-      C* oa = out + (2 * p) * out_line + kb * NB;
+    const int nb_nh = NB * nh;
+#pragma unroll 1
+    for (int p = 0; p < npairs; ++p) {
+      C* oa = out + (2 * p) * out_line;
       C* ob = oa + out_line;
-#pragma unroll
-      for (int c = 0; c < NB; ++c) {
-        const C x = fk[c], y = fm[c];
-        oa[c] = cmk<C>(T(0.5) * (x.x + y.x), T(0.5) * (x.y - y.y));
-        ob[c] = cmk<C>(T(0.5) * (x.y + y.y), T(-0.5) * (x.x - y.x));
+      for (int r = tid; r < nb_nh; r += NT) {
+        const int kb = r / NB;
+        const int cf = p * NB + (r - kb * NB);
+        const C x = sm[kb * SROW + cf];
+        const C y = sm[(kb == 0 ? 0 : L - kb) * SROW + cf];
+        oa[r] = cmk<C>(T(0.5) * (x.x + y.x), T(0.5) * (x.y - y.y));
+        ob[r] = cmk<C>(T(0.5) * (x.y + y.y), T(-0.5) * (x.x - y.x));
       }
     }
+
     // CFL reduction: warp, then block, then one atomic per CTA.
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) vmax = fmax(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
