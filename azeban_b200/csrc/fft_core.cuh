@@ -164,6 +164,57 @@ template <int S, typename C> struct DFT<4, S, C> {
   }
 };
 
+// FP32 butterflies on the paired FP32 pipe of sm_100 (one instruction adds or
+// subtracts both components of a complex value).  a - b is fma(b, -1, a),
+// which rounds exactly as the subtraction does, so results are bit-identical
+// to the scalar forms above.  Multiplications by +-i stay scalar, where the
+// component swap and sign cost nothing.
+__device__ __forceinline__ float2 padd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 psub(float2 a, float2 b) {
+  return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a);
+}
+
+template <int S> struct DFT<2, S, float2> {
+  static __device__ __forceinline__ void run(float2* v) {
+    const float2 a = v[0], b = v[1];
+    v[0] = padd(a, b);
+    v[1] = psub(a, b);
+  }
+};
+
+template <int S> struct DFT<3, S, float2> {
+  static __device__ __forceinline__ void run(float2* v) {
+    const float c = -0.5f;
+    const float s = float(S * 0.8660254037844386467637232);
+    const float2 t1 = padd(v[1], v[2]);
+    const float2 t2 = __ffma2_rn(t1, make_float2(c, c), v[0]);
+    const float2 d = psub(v[1], v[2]);
+    const float2 t3 = make_float2(-s * d.y, s * d.x);  // i * s * d
+    v[0] = padd(v[0], t1);
+    v[1] = padd(t2, t3);
+    v[2] = psub(t2, t3);
+  }
+};
+
+template <int S> struct DFT<4, S, float2> {
+  static __device__ __forceinline__ void run(float2* v) {
+    const float2 a = padd(v[0], v[2]);
+    const float2 b = psub(v[0], v[2]);
+    const float2 c = padd(v[1], v[3]);
+    const float2 t = psub(v[1], v[3]);
+    v[0] = padd(a, c);
+    v[2] = psub(a, c);
+    // d = S i t:  b + d and b - d, componentwise
+    if constexpr (S > 0) {
+      v[1] = make_float2(b.x - t.y, b.y + t.x);
+      v[3] = make_float2(b.x + t.y, b.y - t.x);
+    } else {
+      v[1] = make_float2(b.x + t.y, b.y - t.x);
+      v[3] = make_float2(b.x - t.y, b.y + t.x);
+    }
+  }
+};
+
 // Composite radix R = R1 * R2:  n = R2*n1 + n2, k = k1 + R1*k2.
 template <int R, int S, typename C> struct DFT {
   static constexpr int R1 = Split<R>::R1, R2 = Split<R>::R2;

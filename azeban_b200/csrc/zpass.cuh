@@ -16,6 +16,8 @@
 // (src/azeban/cuda/operations/cufft.cpp:133-149).
 #pragma once
 
+#include <type_traits>
+
 #include "euler_kernels.cuh"
 
 namespace azb {
@@ -92,15 +94,25 @@ template <typename T, int L, int NLP, int DIM, int V> struct ZShape {
   static constexpr int SROW = NFWD + 1;
   static constexpr int TPL = Plan<L, V>::TPL;
   static constexpr int NT = NFWD * TPL;
-  // FP32 std plans: ask for 16 resident warps per SM (a register cap the
-  // compiler meets without spills); wide and FP64 plans need their registers.
-  static constexpr int MINB = (V == 0 && CB == 8) ? (512 + NT - 1) / NT : 1;
+  // FP32: ask for 16 (std plans) or 12 (wide plans) resident warps per SM, a
+  // register cap the compiler meets without spills; FP64 plans need their
+  // registers.
+  static constexpr int MINB = CB != 8 ? 1 : V == 0 ? (512 + NT - 1) / NT : (384 + NT - 1) / NT;
   static constexpr int OFF_TW = 16;
   static constexpr int OFF_WORK = OFF_TW + L * CB;
   static constexpr int OFF_IN = OFF_WORK + ((L * SROW * CB + 15) / 16) * 16;
   // complex elements of one chunk's input
   static __host__ __device__ long long chunk_elems(int nh) { return 2LL * NLP * nh * DIM; }
   static __host__ __device__ long long smem_bytes(int nh) { return OFF_IN + chunk_elems(nh) * CB; }
+};
+
+// Plan of the inverse transforms: the velocity columns are DIM/NB of the
+// product columns, so with the wide plan half (3-D) of the CTA would sit out
+// the inverse phase.  The std plan runs more threads per column; take it when
+// the CTA has the threads for it, so the inverse phase spreads over the CTA.
+template <int L, int V, int NCOL, int NT> struct InvPlan {
+  static constexpr bool kStd = V == 1 && NCOL * Plan<L, 0>::TPL <= NT && Plan<L, 0>::TPL > Plan<L, 1>::TPL;
+  using type = typename std::conditional<kStd, Plan<L, 0>, Plan<L, V>>::type;
 };
 
 template <typename T, int L, int NLP, int DIM, int V>
@@ -187,10 +199,11 @@ __global__ void __launch_bounds__(ZShape<T, L, NLP, DIM, V>::NT, ZShape<T, L, NL
 
     // 2. Inverse transforms of the velocity columns, in place.
     {
-      const bool active = tid < NINV * TPL;
+      using PI = typename InvPlan<L, V, NINV, NT>::type;
+      const bool active = tid < NINV * PI::TPL;
       const int col = VOFF + (active ? tid % NINV : 0);
       const int tl = active ? tid / NINV : 0;
-      fft_columns<C, +1, L, SROW, true, P>(
+      fft_columns<C, +1, L, SROW, true, PI>(
           sm, tw, col, tl, [&](int m) { return sm[m * SROW + col]; },
           [&](int m, C v) { sm[m * SROW + col] = v; }, active);
     }
