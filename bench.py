@@ -250,8 +250,11 @@ def run_ours(args, rank, world, local):
     nl = (ct.c_longlong * 5)()
     _lib.check(_lib.lib.az_profile_read(ms, by, nl, 5))
     pass_names = ["inv_x_pad", "inv_y_pad", "z_product", "fwd_y_trunc", "fwd_x_epilogue"]
-    kernel_keys = ["k_cols_pad_inv_x", "k_cols_pad_inv_y", "k_rows_product", "k_cols_trunc_fwd",
-                   "k_fwd_epilogue"]
+    # The product pass runs k_zpass when bit 1 of its tuned variant is set.
+    zv = ct.c_int()
+    _lib.check(_lib.lib.az_tune_get(1, g.N_phys_pad, 1, ct.byref(zv)))
+    kernel_keys = ["k_cols_pad_inv_x", "k_cols_pad_inv_y", "k_zpass" if zv.value & 2 else "k_rows_product",
+                   "k_cols_trunc_fwd", "k_fwd_epilogue"]
     peak, peak_kind = measured_peak_hbm()
     passes = {}
     for i, nm in enumerate(pass_names):
