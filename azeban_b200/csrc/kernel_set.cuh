@@ -129,7 +129,7 @@ template <typename T, int L, int V> struct LaunchV {
     using Z = ZShape<T, L, NLP, DIM, V>;
     auto k = k_zpass<T, L, NLP, DIM, V>;
     const long long smem = Z::smem_bytes(a.nh);
-    if (smem > 227 * 1024) return cudaErrorInvalidValue;
+    if (smem < 0 || smem > 227 * 1024) return cudaErrorInvalidValue;
     // The bulk copy needs a 16-byte aligned chunk of whole line pairs.
     const long long lb = (long long)a.nh * DIM * Z::CB;
     if ((reinterpret_cast<uintptr_t>(a.in) & 15) != 0 || (2 * lb) % 16 != 0 ||

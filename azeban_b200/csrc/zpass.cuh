@@ -79,19 +79,20 @@ struct ZArgs {
 };
 
 // Shared-memory layout of one CTA (bytes), shared by the kernel and its
-// launcher: the mbarrier, the twiddle table, the work area [L][SROW] and the
-// chunk's input.  Work columns [0, NFWD) hold the
-// product transforms; the velocity transforms sit at the end of the same
-// rows, columns [VOFF, NFWD).  The product columns of pair p overlap only
-// velocity columns of pairs <= p, so a thread that owns a row and handles its
-// pairs in order writes the products in place, after reading what they cover.
+// launcher: the mbarrier, the twiddle table, the product region P [L][SP]
+// and the velocity region V [L][SV].  The chunk's input is copied into P,
+// which is dead until the products are written.  The row strides equal the
+// column counts (24 and 12 for 3-D pairs of four): with columns fastest in
+// the transform's thread mapping, a half-warp then covers whole rows or two
+// rows whose banks do not collide, and the row-wise phases map lanes across
+// pairs as well as rows.
 template <typename T, int L, int NLP, int DIM, int V> struct ZShape {
   static constexpr int CB = int(sizeof(cvec<T>));
   static constexpr int NB = DIM * (DIM + 1) / 2;
   static constexpr int NINV = DIM * NLP;
   static constexpr int NFWD = NB * NLP;
-  static constexpr int VOFF = NFWD - NINV;
-  static constexpr int SROW = NFWD + 1;
+  static constexpr int SP = NFWD;
+  static constexpr int SV = NINV;
   static constexpr int TPL = Plan<L, V>::TPL;
   static constexpr int NT = NFWD * TPL;
   // FP32: ask for 16 (std plans) or 12 (wide plans) resident warps per SM, a
@@ -99,11 +100,14 @@ template <typename T, int L, int NLP, int DIM, int V> struct ZShape {
   // registers.
   static constexpr int MINB = CB != 8 ? 1 : V == 0 ? (512 + NT - 1) / NT : (384 + NT - 1) / NT;
   static constexpr int OFF_TW = 16;
-  static constexpr int OFF_WORK = OFF_TW + L * CB;
-  static constexpr int OFF_IN = OFF_WORK + ((L * SROW * CB + 15) / 16) * 16;
-  // complex elements of one chunk's input
+  static constexpr int OFF_P = OFF_TW + L * CB;
+  static constexpr int OFF_V = OFF_P + ((L * SP * CB + 15) / 16) * 16;
+  static constexpr int BYTES = OFF_V + L * SV * CB;
+  // complex elements of one chunk's input (must fit in P: 2 nh DIM <= L NB)
   static __host__ __device__ long long chunk_elems(int nh) { return 2LL * NLP * nh * DIM; }
-  static __host__ __device__ long long smem_bytes(int nh) { return OFF_IN + chunk_elems(nh) * CB; }
+  static __host__ __device__ long long smem_bytes(int nh) {
+    return chunk_elems(nh) <= (long long)L * SP ? BYTES : -1;
+  }
 };
 
 // Plan of the inverse transforms: the velocity columns are DIM/NB of the
@@ -124,15 +128,15 @@ __global__ void __launch_bounds__(ZShape<T, L, NLP, DIM, V>::NT, ZShape<T, L, NL
   constexpr int NB = Z::NB;
   constexpr int NINV = Z::NINV;
   constexpr int NFWD = Z::NFWD;
-  constexpr int SROW = Z::SROW;
-  constexpr int VOFF = Z::VOFF;
-  constexpr int TPL = Z::TPL;
+  constexpr int SP = Z::SP;
+  constexpr int SV = Z::SV;
   constexpr int NT = Z::NT;
   extern __shared__ __align__(16) unsigned char az_smem[];
   unsigned long long* bar = reinterpret_cast<unsigned long long*>(az_smem);
   C* tw = reinterpret_cast<C*>(az_smem + Z::OFF_TW);
-  C* sm = reinterpret_cast<C*>(az_smem + Z::OFF_WORK);
-  const C* cin = reinterpret_cast<const C*>(az_smem + Z::OFF_IN);
+  C* pw = reinterpret_cast<C*>(az_smem + Z::OFF_P);
+  C* vw = reinterpret_cast<C*>(az_smem + Z::OFF_V);
+  const C* cin = pw;  // the chunk's input, until the products overwrite it
   const int member = blockIdx.y;
   Ctrl* ctrl = a.ctrl + member;
   if (ctrl->skip) return;
@@ -150,8 +154,7 @@ __global__ void __launch_bounds__(ZShape<T, L, NLP, DIM, V>::NT, ZShape<T, L, NL
     mbar_fence_init();
     const unsigned bytes = unsigned(2 * npairs * in_line * Z::CB);
     mbar_expect_tx(&bar[0], bytes);
-    bulk_load(az_smem + Z::OFF_IN,
-              reinterpret_cast<const C*>(a.in) + member * a.in_mem + line0 * in_line, bytes, &bar[0]);
+    bulk_load(pw, reinterpret_cast<const C*>(a.in) + member * a.in_mem + line0 * in_line, bytes, &bar[0]);
   }
   load_twiddles<C, L>(tw, reinterpret_cast<const C*>(a.tw));
   __syncthreads();
@@ -163,126 +166,115 @@ __global__ void __launch_bounds__(ZShape<T, L, NLP, DIM, V>::NT, ZShape<T, L, NL
   T vmax = T(0);
   bool bad = false;
 
-    // 1. Hermitian extension into the velocity columns: column (pair p, slot
-    //    q) holds signal 2q + i * signal 2q+1, signal s = component s % DIM of
-    //    line s / DIM of the pair.  Bin k < nh gives rows k and L - k; rows
-    //    [nh, L - nh] are zero.  The imaginary parts of bin 0 and bin L/2 are
-    //    dropped, as a c2r does.
-    for (int idx = tid; idx < NLP * nh; idx += NT) {
-      const int p = idx / nh;
-      const int kb = idx - p * nh;
-      C sg[2 * DIM];
-      const C* src = cin + (2 * p) * in_line + kb * DIM;
+  // 1. Hermitian extension into V: column (pair p, slot q) holds signal 2q +
+  //    i * signal 2q+1, signal s = component s % DIM of line s / DIM of the
+  //    pair.  Bin k < nh gives rows k and L - k; rows [nh, L - nh] are zero.
+  //    The imaginary parts of bin 0 and bin L/2 are dropped, as a c2r does.
+  //    Lanes run over pairs fastest, then bins.
+  for (int idx = tid; idx < NLP * nh; idx += NT) {
+    const int kb = idx / NLP;
+    const int p = idx - kb * NLP;
+    C sg[2 * DIM];
+    const C* src = cin + (2 * p) * in_line + kb * DIM;
 #pragma unroll
-      for (int s = 0; s < 2 * DIM; ++s)
-        sg[s] = p < npairs ? src[(s / DIM) * in_line + s % DIM] : cmk<C>(T(0), T(0));
-      const bool edge = kb == 0 || 2 * kb == L;
-      if (edge) {
+    for (int s = 0; s < 2 * DIM; ++s)
+      sg[s] = p < npairs ? src[(s / DIM) * in_line + s % DIM] : cmk<C>(T(0), T(0));
+    const bool edge = kb == 0 || 2 * kb == L;
+    if (edge) {
 #pragma unroll
-        for (int s = 0; s < 2 * DIM; ++s) sg[s].y = T(0);
-      }
-      C* row = sm + kb * SROW + VOFF + p * DIM;
-      C* mrow = sm + (L - kb) * SROW + VOFF + p * DIM;
-#pragma unroll
-      for (int q = 0; q < DIM; ++q) {
-        const C x = sg[2 * q], y = sg[2 * q + 1];
-        row[q] = cmk<C>(x.x - y.y, x.y + y.x);
-        if (!edge) mrow[q] = cmk<C>(x.x + y.y, y.x - x.y);
-      }
+      for (int s = 0; s < 2 * DIM; ++s) sg[s].y = T(0);
     }
-    for (int idx = tid; idx < (L - 2 * nh + 1) * NINV; idx += NT) {
-      const int r = idx / NINV;
-      const int c = idx - r * NINV;
-      sm[(nh + r) * SROW + VOFF + c] = cmk<C>(T(0), T(0));
+    C* row = vw + kb * SV + p * DIM;
+    C* mrow = vw + (L - kb) * SV + p * DIM;
+#pragma unroll
+    for (int q = 0; q < DIM; ++q) {
+      const C x = sg[2 * q], y = sg[2 * q + 1];
+      row[q] = cmk<C>(x.x - y.y, x.y + y.x);
+      if (!edge) mrow[q] = cmk<C>(x.x + y.y, y.x - x.y);
     }
-    __syncthreads();
+  }
+  for (int idx = tid; idx < (L - 2 * nh + 1) * NINV; idx += NT) vw[nh * SV + idx] = cmk<C>(T(0), T(0));
+  __syncthreads();
 
-    // 2. Inverse transforms of the velocity columns, in place.
-    {
-      using PI = typename InvPlan<L, V, NINV, NT>::type;
-      const bool active = tid < NINV * PI::TPL;
-      const int col = VOFF + (active ? tid % NINV : 0);
-      const int tl = active ? tid / NINV : 0;
-      fft_columns<C, +1, L, SROW, true, PI>(
-          sm, tw, col, tl, [&](int m) { return sm[m * SROW + col]; },
-          [&](int m, C v) { sm[m * SROW + col] = v; }, active);
-    }
-    __syncthreads();
+  // 2. Inverse transforms of the velocity columns, in place in V.
+  {
+    using PI = typename InvPlan<L, V, NINV, NT>::type;
+    const bool active = tid < NINV * PI::TPL;
+    const int col = active ? tid % NINV : 0;
+    const int tl = active ? tid / NINV : 0;
+    fft_columns<C, +1, L, SV, true, PI>(
+        vw, tw, col, tl, [&](int m) { return vw[m * SV + col]; },
+        [&](int m, C v) { vw[m * SV + col] = v; }, active);
+  }
+  __syncthreads();
 
-    // 3. CFL maximum and products B = u (x) u in the reference's component
-    //    order (product c of line a in the real part, of line b in the
-    //    imaginary part), in place: a thread owns rows and handles the pairs
-    //    of a row in order.
-    const T norm = T(a.norm);
+  // 3. CFL maximum and products B = u (x) u in the reference's component
+  //    order (product c of line a in the real part, of line b in the
+  //    imaginary part), from V into P.  Lanes run over pairs fastest.
+  const T norm = T(a.norm);
+  for (int idx = tid; idx < L * NLP; idx += NT) {
+    const int m = idx / NLP;
+    const int p = idx - m * NLP;
+    const C* v = vw + m * SV + p * DIM;
+    T u[2 * DIM];
 #pragma unroll
-    for (int it = 0; it < (L + NT - 1) / NT; ++it) {
-      const int m = tid + it * NT;
-      if (L % NT != 0 && m >= L) break;
-#pragma unroll
-      for (int p = 0; p < NLP; ++p) {
-        {
-          const C* v = sm + m * SROW + VOFF + p * DIM;
-          T u[2 * DIM];
-#pragma unroll
-          for (int q = 0; q < DIM; ++q) {
-            const C z = v[q];
-            u[2 * q] = z.x;
-            u[2 * q + 1] = z.y;
-          }
-#pragma unroll
-          for (int s = 0; s < 2 * DIM; ++s) {
-            const T av = fabs(u[s]);
-            bad |= !(av <= kFiniteMax<T>);
-            vmax = fmax(vmax, av);
-            u[s] *= norm;
-          }
-          C* w = sm + m * SROW + p * NB;
-          if constexpr (DIM == 2) {
-            w[0] = cmk<C>(u[0] * u[0], u[2] * u[2]);
-            w[1] = cmk<C>(u[0] * u[1], u[2] * u[3]);
-            w[2] = cmk<C>(u[1] * u[1], u[3] * u[3]);
-          } else {
-            w[0] = cmk<C>(u[0] * u[0], u[3] * u[3]);
-            w[1] = cmk<C>(u[1] * u[0], u[4] * u[3]);
-            w[2] = cmk<C>(u[1] * u[1], u[4] * u[4]);
-            w[3] = cmk<C>(u[2] * u[0], u[5] * u[3]);
-            w[4] = cmk<C>(u[2] * u[1], u[5] * u[4]);
-            w[5] = cmk<C>(u[2] * u[2], u[5] * u[5]);
-          }
-        }
-      }
+    for (int q = 0; q < DIM; ++q) {
+      const C z = v[q];
+      u[2 * q] = z.x;
+      u[2 * q + 1] = z.y;
     }
-    __syncthreads();
-
-    // 4. Forward transforms of the NFWD product columns.
-    {
-      const int col = tid % NFWD;
-      const int tl = tid / NFWD;
-      fft_columns<C, -1, L, SROW, true, P>(
-          sm, tw, col, tl, [&](int m) { return sm[m * SROW + col]; },
-          [&](int m, C v) { sm[m * SROW + col] = v; });
+#pragma unroll
+    for (int s = 0; s < 2 * DIM; ++s) {
+      const T av = fabs(u[s]);
+      bad |= !(av <= kFiniteMax<T>);
+      vmax = fmax(vmax, av);
+      u[s] *= norm;
     }
-    __syncthreads();
+    C* w = pw + m * SP + p * NB;
+    if constexpr (DIM == 2) {
+      w[0] = cmk<C>(u[0] * u[0], u[2] * u[2]);
+      w[1] = cmk<C>(u[0] * u[1], u[2] * u[3]);
+      w[2] = cmk<C>(u[1] * u[1], u[3] * u[3]);
+    } else {
+      w[0] = cmk<C>(u[0] * u[0], u[3] * u[3]);
+      w[1] = cmk<C>(u[1] * u[0], u[4] * u[3]);
+      w[2] = cmk<C>(u[1] * u[1], u[4] * u[4]);
+      w[3] = cmk<C>(u[2] * u[0], u[5] * u[3]);
+      w[4] = cmk<C>(u[2] * u[1], u[5] * u[4]);
+      w[5] = cmk<C>(u[2] * u[2], u[5] * u[5]);
+    }
+  }
+  __syncthreads();
 
-    // 5. Separate the two real spectra and write bins [0, nh), component
-    //    fastest, so consecutive threads store consecutive elements of a line.
-    C* out = reinterpret_cast<C*>(a.out) + member * a.out_mem + line0 * out_line;
-    const int nb_nh = NB * nh;
+  // 4. Forward transforms of the NFWD product columns, in place in P.
+  {
+    const int col = tid % NFWD;
+    const int tl = tid / NFWD;
+    fft_columns<C, -1, L, SP, true, P>(
+        pw, tw, col, tl, [&](int m) { return pw[m * SP + col]; },
+        [&](int m, C v) { pw[m * SP + col] = v; });
+  }
+  __syncthreads();
+
+  // 5. Separate the two real spectra and write bins [0, nh), component
+  //    fastest, so consecutive threads store consecutive elements of a line.
+  C* out = reinterpret_cast<C*>(a.out) + member * a.out_mem + line0 * out_line;
+  const int nb_nh = NB * nh;
 #pragma unroll 1
-    for (int p = 0; p < npairs; ++p) {
-      C* oa = out + (2 * p) * out_line;
-      C* ob = oa + out_line;
-      for (int r = tid; r < nb_nh; r += NT) {
-        const int kb = r / NB;
-        const int cf = p * NB + (r - kb * NB);
-        const C x = sm[kb * SROW + cf];
-        const C y = sm[(kb == 0 ? 0 : L - kb) * SROW + cf];
-        oa[r] = cmk<C>(T(0.5) * (x.x + y.x), T(0.5) * (x.y - y.y));
-        ob[r] = cmk<C>(T(0.5) * (x.y + y.y), T(-0.5) * (x.x - y.x));
-      }
+  for (int p = 0; p < npairs; ++p) {
+    C* oa = out + (2 * p) * out_line;
+    C* ob = oa + out_line;
+    for (int r = tid; r < nb_nh; r += NT) {
+      const int kb = r / NB;
+      const int cf = p * NB + (r - kb * NB);
+      const C x = pw[kb * SP + cf];
+      const C y = pw[(kb == 0 ? 0 : L - kb) * SP + cf];
+      oa[r] = cmk<C>(T(0.5) * (x.x + y.x), T(0.5) * (x.y - y.y));
+      ob[r] = cmk<C>(T(0.5) * (x.y + y.y), T(-0.5) * (x.x - y.x));
     }
+  }
 
-    // CFL reduction: warp, then block, then one atomic per CTA.
+  // CFL reduction: warp, then block, then one atomic per CTA.
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) vmax = fmax(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
   const unsigned anybad = __any_sync(0xffffffffu, bad);
