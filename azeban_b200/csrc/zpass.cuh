@@ -79,20 +79,28 @@ struct ZArgs {
 };
 
 // Shared-memory layout of one CTA (bytes), shared by the kernel and its
-// launcher: the mbarrier, the twiddle table, the product region P [L][SP]
-// and the velocity region V [L][SV].  The chunk's input is copied into P,
-// which is dead until the products are written.  The row strides equal the
-// column counts (24 and 12 for 3-D pairs of four): with columns fastest in
-// the transform's thread mapping, a half-warp then covers whole rows or two
-// rows whose banks do not collide, and the row-wise phases map lanes across
-// pairs as well as rows.
+// launcher: the mbarrier, the twiddle table, the product columns P and the
+// velocity columns V.  Two layouts, by element size:
+//  - FP32 (REGIONS): P [L][NFWD] and V [L][NINV] are separate regions whose
+//    row strides equal their column counts (24 and 12 for 3-D pairs of
+//    four).  With columns fastest in the transform's thread mapping a
+//    half-warp then covers whole rows, or two rows whose banks do not
+//    collide, and the row-wise phases map lanes across pairs as well as
+//    rows.  The chunk's input is copied into P, dead until the products.
+//  - FP64: one work area [L][NFWD + 1]; P is columns [0, NFWD), V the last
+//    NINV of them (VOFF).  The product columns of pair p overlap only
+//    velocity columns of pairs <= p, so a thread that owns a row and handles
+//    its pairs in order writes the products in place.  The input has its
+//    own buffer.  (Measured faster for 16-byte elements.)
 template <typename T, int L, int NLP, int DIM, int V> struct ZShape {
   static constexpr int CB = int(sizeof(cvec<T>));
+  static constexpr bool REGIONS = CB == 8;
   static constexpr int NB = DIM * (DIM + 1) / 2;
   static constexpr int NINV = DIM * NLP;
   static constexpr int NFWD = NB * NLP;
-  static constexpr int SP = NFWD;
-  static constexpr int SV = NINV;
+  static constexpr int SP = REGIONS ? NFWD : NFWD + 1;
+  static constexpr int SV = REGIONS ? NINV : NFWD + 1;
+  static constexpr int VOFF = REGIONS ? 0 : NFWD - NINV;
   static constexpr int TPL = Plan<L, V>::TPL;
   static constexpr int NT = NFWD * TPL;
   // FP32: ask for 16 (std plans) or 12 (wide plans) resident warps per SM, a
@@ -101,12 +109,16 @@ template <typename T, int L, int NLP, int DIM, int V> struct ZShape {
   static constexpr int MINB = CB != 8 ? 1 : V == 0 ? (512 + NT - 1) / NT : (384 + NT - 1) / NT;
   static constexpr int OFF_TW = 16;
   static constexpr int OFF_P = OFF_TW + L * CB;
-  static constexpr int OFF_V = OFF_P + ((L * SP * CB + 15) / 16) * 16;
-  static constexpr int BYTES = OFF_V + L * SV * CB;
-  // complex elements of one chunk's input (must fit in P: 2 nh DIM <= L NB)
+  static constexpr int P_BYTES = ((L * SP * CB + 15) / 16) * 16;
+  static constexpr int OFF_V = REGIONS ? OFF_P + P_BYTES : OFF_P + VOFF * CB;
+  static constexpr int OFF_IN = REGIONS ? OFF_P : OFF_P + P_BYTES;
+  static constexpr int BYTES = REGIONS ? OFF_V + L * SV * CB : OFF_IN;
+  // complex elements of one chunk's input
   static __host__ __device__ long long chunk_elems(int nh) { return 2LL * NLP * nh * DIM; }
+  // -1 when the input does not fit in P (REGIONS), which holds it
   static __host__ __device__ long long smem_bytes(int nh) {
-    return chunk_elems(nh) <= (long long)L * SP ? BYTES : -1;
+    if (REGIONS) return chunk_elems(nh) <= (long long)L * SP ? BYTES : -1;
+    return BYTES + chunk_elems(nh) * CB;
   }
 };
 
@@ -136,7 +148,7 @@ __global__ void __launch_bounds__(ZShape<T, L, NLP, DIM, V>::NT, ZShape<T, L, NL
   C* tw = reinterpret_cast<C*>(az_smem + Z::OFF_TW);
   C* pw = reinterpret_cast<C*>(az_smem + Z::OFF_P);
   C* vw = reinterpret_cast<C*>(az_smem + Z::OFF_V);
-  const C* cin = pw;  // the chunk's input, until the products overwrite it
+  const C* cin = reinterpret_cast<const C*>(az_smem + Z::OFF_IN);
   const int member = blockIdx.y;
   Ctrl* ctrl = a.ctrl + member;
   if (ctrl->skip) return;
@@ -154,7 +166,8 @@ __global__ void __launch_bounds__(ZShape<T, L, NLP, DIM, V>::NT, ZShape<T, L, NL
     mbar_fence_init();
     const unsigned bytes = unsigned(2 * npairs * in_line * Z::CB);
     mbar_expect_tx(&bar[0], bytes);
-    bulk_load(pw, reinterpret_cast<const C*>(a.in) + member * a.in_mem + line0 * in_line, bytes, &bar[0]);
+    bulk_load(az_smem + Z::OFF_IN, reinterpret_cast<const C*>(a.in) + member * a.in_mem + line0 * in_line,
+              bytes, &bar[0]);
   }
   load_twiddles<C, L>(tw, reinterpret_cast<const C*>(a.tw));
   __syncthreads();
@@ -170,10 +183,10 @@ __global__ void __launch_bounds__(ZShape<T, L, NLP, DIM, V>::NT, ZShape<T, L, NL
   //    i * signal 2q+1, signal s = component s % DIM of line s / DIM of the
   //    pair.  Bin k < nh gives rows k and L - k; rows [nh, L - nh] are zero.
   //    The imaginary parts of bin 0 and bin L/2 are dropped, as a c2r does.
-  //    Lanes run over pairs fastest, then bins.
+  //    REGIONS: lanes run over pairs fastest, then bins; else over bins.
   for (int idx = tid; idx < NLP * nh; idx += NT) {
-    const int kb = idx / NLP;
-    const int p = idx - kb * NLP;
+    const int kb = Z::REGIONS ? idx / NLP : idx % nh;
+    const int p = Z::REGIONS ? idx % NLP : idx / nh;
     C sg[2 * DIM];
     const C* src = cin + (2 * p) * in_line + kb * DIM;
 #pragma unroll
@@ -193,7 +206,10 @@ __global__ void __launch_bounds__(ZShape<T, L, NLP, DIM, V>::NT, ZShape<T, L, NL
       if (!edge) mrow[q] = cmk<C>(x.x + y.y, y.x - x.y);
     }
   }
-  for (int idx = tid; idx < (L - 2 * nh + 1) * NINV; idx += NT) vw[nh * SV + idx] = cmk<C>(T(0), T(0));
+  for (int idx = tid; idx < (L - 2 * nh + 1) * NINV; idx += NT) {
+    const int r = idx / NINV;
+    vw[(nh + r) * SV + (idx - r * NINV)] = cmk<C>(T(0), T(0));
+  }
   __syncthreads();
 
   // 2. Inverse transforms of the velocity columns, in place in V.
@@ -210,11 +226,11 @@ __global__ void __launch_bounds__(ZShape<T, L, NLP, DIM, V>::NT, ZShape<T, L, NL
 
   // 3. CFL maximum and products B = u (x) u in the reference's component
   //    order (product c of line a in the real part, of line b in the
-  //    imaginary part), from V into P.  Lanes run over pairs fastest.
+  //    imaginary part), from V into P.  REGIONS: lanes run over pairs
+  //    fastest.  Else a thread owns a row and handles its pairs in order
+  //    (each pair's products overwrite only velocity columns already read).
   const T norm = T(a.norm);
-  for (int idx = tid; idx < L * NLP; idx += NT) {
-    const int m = idx / NLP;
-    const int p = idx - m * NLP;
+  auto product = [&](int m, int p) {
     const C* v = vw + m * SV + p * DIM;
     T u[2 * DIM];
 #pragma unroll
@@ -242,6 +258,14 @@ __global__ void __launch_bounds__(ZShape<T, L, NLP, DIM, V>::NT, ZShape<T, L, NL
       w[3] = cmk<C>(u[2] * u[0], u[5] * u[3]);
       w[4] = cmk<C>(u[2] * u[1], u[5] * u[4]);
       w[5] = cmk<C>(u[2] * u[2], u[5] * u[5]);
+    }
+  };
+  if constexpr (Z::REGIONS) {
+    for (int idx = tid; idx < L * NLP; idx += NT) product(idx / NLP, idx % NLP);
+  } else {
+    for (int m = tid; m < L; m += NT) {
+#pragma unroll
+      for (int p = 0; p < NLP; ++p) product(m, p);
     }
   }
   __syncthreads();
