@@ -325,29 +325,31 @@ struct EpiArgs {
 };
 
 // nu(|k|) of the reference's viscosity laws
-// (include/azeban/equations/spectral_viscosity.hpp:27-123).
-template <typename T> __device__ __forceinline__ T visc_eval(const Visc& v, T k) {
+// (include/azeban/equations/spectral_viscosity.hpp:27-123), evaluated from
+// |k|^2: SmoothCutoff1D takes (|k|/k0)^2 = |k|^2 / k0^2 and Quadratic
+// (|k|/2 pi)^2 = |k|^2 / (2 pi)^2, so neither needs the square root.  Step1D
+// compares |k| > k0 as the reference does, on the square root.
+template <typename T> __device__ __forceinline__ T visc_from_k2(const Visc& v, T absk2, T inv_k0sq) {
   switch (v.type) {
-    case VISC_SMOOTH_CUTOFF:
+    case VISC_SMOOTH_CUTOFF: {
+      const T k2 = absk2 * inv_k0sq;
+      const T k4 = k2 * k2;
+      const T k8 = k4 * k4;
+      const T k16 = k8 * k8;
+      const T k18 = k16 * k2;
+      const T q = T(1) - exp(-k18);
+      const T pk = (v.s == 1.0) ? absk2 : T(pow(absk2, T(v.s)));
+      return -T(v.eps) * pk * q;
+    }
     case VISC_STEP: {
-      T q;
-      if (v.type == VISC_SMOOTH_CUTOFF) {
-        const T k1 = fabs(k) / T(v.k0);
-        const T k2 = k1 * k1;
-        const T k4 = k2 * k2;
-        const T k8 = k4 * k4;
-        const T k16 = k8 * k8;
-        const T k18 = k16 * k2;
-        q = T(1) - exp(-k18);
-      } else {
-        q = fabs(k) > T(v.k0) ? T(1) : T(0);
-      }
+      const T k = sqrt(absk2);
+      const T q = k > T(v.k0) ? T(1) : T(0);
       const T pk = (v.s == 1.0) ? k * k : T(pow(k, T(2 * v.s)));
       return -T(v.eps) * pk * q;
     }
     case VISC_QUADRATIC: {
-      const T knorm = k / T(2 * 3.14159265358979323846);
-      return -T(v.eps) * fmax(T(0), knorm * knorm - T(v.N));
+      const T kn2 = absk2 * T(1.0 / (4 * 3.14159265358979323846 * 3.14159265358979323846));
+      return -T(v.eps) * fmax(T(0), kn2 - T(v.N));
     }
     default:
       return T(0);
@@ -409,12 +411,25 @@ __global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NCM * Plan<L, V>::TPL)
   const C* u0 = reinterpret_cast<const C*>(a.u0) + member * a.u_mem;
   C* out = reinterpret_cast<C*>(a.out) + member * a.u_mem;
   const int u_row = int(a.u_row), u_comp = int(a.u_comp);  // a member's state < 2^31 elements
-  for (int idx = tid; idx < N * NCM; idx += NT) {
-    const int pl = idx % NCM;
-    const int i = idx / NCM;
-    const int p = tile * NCM + pl;
-    if (p >= a.ninner) continue;
+  const T inv_k0sq = T(1.0 / (a.visc.k0 * a.visc.k0));
+  // NT is a multiple of NCM, so a thread keeps one mode column pl (and its
+  // second and third wavenumbers) and walks the retained rows i.
+  const int pl = tid % NCM;
+  const int p = tile * NCM + pl;
+  if (p >= a.ninner) return;
+  T k2, k3;
+  if constexpr (DIM == 2) {
+    k2 = twopi * T(p);
+    k3 = T(0);
+  } else {
+    const int j = p / a.nh;
+    const int kk = p - j * a.nh;
+    k2 = twopi * T(j >= N / 2 + 1 ? j - N : j);
+    k3 = twopi * T(kk);
+  }
+  for (int i = tid / NCM; i < N; i += NT / NCM) {
     const int i_ = i >= N / 2 + 1 ? i - N : i;
+    const T k1 = twopi * T(i_);
     C Bv[NB];
 #pragma unroll
     for (int c = 0; c < NB; ++c) Bv[c] = sm[i * SROW + pl * NB + c];
@@ -422,28 +437,18 @@ __global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NCM * Plan<L, V>::TPL)
     C uv[DIM];
 #pragma unroll
     for (int c = 0; c < DIM; ++c) uv[c] = u[c * u_comp + off];
+    // b = i k.B (force = 0), then L = b - k (k.b) / |k|^2
     C Lh[DIM];
     T absk2;
     if constexpr (DIM == 2) {
-      const int kk = (int)p;
-      const T k1 = twopi * T(i_);
-      const T k2 = twopi * T(kk);
       absk2 = k1 * k1 + k2 * k2;
-      // b = i k.B (force = 0)
       const C b1 = cmk<C>(-k1 * Bv[0].y - k2 * Bv[1].y, k1 * Bv[0].x + k2 * Bv[1].x);
       const C b2 = cmk<C>(-k1 * Bv[1].y - k2 * Bv[2].y, k1 * Bv[1].x + k2 * Bv[2].x);
       const T inv = T(1) / absk2;
-      const T k11 = k1 * k1 * inv, k12 = k1 * k2 * inv, k22 = k2 * k2 * inv;
-      const T c11 = T(1) - k11, c12 = T(0) - k12, c22 = T(1) - k22;
-      Lh[0] = cmk<C>(c11 * b1.x + c12 * b2.x, c11 * b1.y + c12 * b2.y);
-      Lh[1] = cmk<C>(c12 * b1.x + c22 * b2.x, c12 * b1.y + c22 * b2.y);
+      const C sk = cmk<C>((k1 * b1.x + k2 * b2.x) * inv, (k1 * b1.y + k2 * b2.y) * inv);
+      Lh[0] = cmk<C>(b1.x - k1 * sk.x, b1.y - k1 * sk.y);
+      Lh[1] = cmk<C>(b2.x - k2 * sk.x, b2.y - k2 * sk.y);
     } else {
-      const int j = p / a.nh;
-      const int kk = p - j * a.nh;
-      const int j_ = j >= N / 2 + 1 ? j - N : j;
-      const T k1 = twopi * T(i_);
-      const T k2 = twopi * T(j_);
-      const T k3 = twopi * T(kk);
       absk2 = k1 * k1 + k2 * k2 + k3 * k3;
       // B order: 0 B11, 1 B21, 2 B22, 3 B31, 4 B32, 5 B33
       const C b1 = cmk<C>(-k1 * Bv[0].y - k2 * Bv[1].y - k3 * Bv[3].y,
@@ -453,15 +458,12 @@ __global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NCM * Plan<L, V>::TPL)
       const C b3 = cmk<C>(-k1 * Bv[3].y - k2 * Bv[4].y - k3 * Bv[5].y,
                           k1 * Bv[3].x + k2 * Bv[4].x + k3 * Bv[5].x);
       const T inv = T(1) / absk2;
-      const T k11 = k1 * k1 * inv, k12 = k1 * k2 * inv, k13 = k1 * k3 * inv;
-      const T k22 = k2 * k2 * inv, k23 = k2 * k3 * inv, k33 = k3 * k3 * inv;
-      const T c11 = T(1) - k11, c12 = T(0) - k12, c13 = T(0) - k13;
-      const T c22 = T(1) - k22, c23 = T(0) - k23, c33 = T(1) - k33;
-      Lh[0] = cmk<C>(c11 * b1.x + c12 * b2.x + c13 * b3.x, c11 * b1.y + c12 * b2.y + c13 * b3.y);
-      Lh[1] = cmk<C>(c12 * b1.x + c22 * b2.x + c23 * b3.x, c12 * b1.y + c22 * b2.y + c23 * b3.y);
-      Lh[2] = cmk<C>(c13 * b1.x + c23 * b2.x + c33 * b3.x, c13 * b1.y + c23 * b2.y + c33 * b3.y);
+      const C sk = cmk<C>((k1 * b1.x + k2 * b2.x + k3 * b3.x) * inv, (k1 * b1.y + k2 * b2.y + k3 * b3.y) * inv);
+      Lh[0] = cmk<C>(b1.x - k1 * sk.x, b1.y - k1 * sk.y);
+      Lh[1] = cmk<C>(b2.x - k2 * sk.x, b2.y - k2 * sk.y);
+      Lh[2] = cmk<C>(b3.x - k3 * sk.x, b3.y - k3 * sk.y);
     }
-    const T nu = visc_eval<T>(a.visc, sqrt(absk2));
+    const T nu = visc_from_k2<T>(a.visc, absk2, inv_k0sq);
     const bool zero = absk2 == T(0);
 #pragma unroll
     for (int c = 0; c < DIM; ++c) {
