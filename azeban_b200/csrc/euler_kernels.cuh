@@ -90,8 +90,6 @@ __global__ void __launch_bounds__(NC * Plan<L, V>::TPL) k_cols(ColArgs a) {
   const C* in = reinterpret_cast<const C*>(a.in) + member * a.in_mem + outer * a.in_outer + pin;
   C* out = reinterpret_cast<C*>(a.out) + member * a.out_mem + comp * a.out_comp +
            outer * a.out_outer + p;
-  load_twiddles<C, L>(tw, reinterpret_cast<const C*>(a.tw));
-  __syncthreads();
   const int n = a.n_short;
   // Row offsets fit 32 bits (the launcher checks L * stride < 2^31).
   const int in_row = int(a.in_row);
@@ -107,7 +105,13 @@ __global__ void __launch_bounds__(NC * Plan<L, V>::TPL) k_cols(ColArgs a) {
     if constexpr (MODE == COL_TRUNC) dst = retained_row(m, n, L);
     if (valid && dst >= 0) out[dst * out_row] = v;
   };
-  fft_columns<C, S, L, NC, false, P>(sm, tw, col, tl, load, store);
+  // The first-stage loads go out before the twiddle table is fetched, so the
+  // two global round trips overlap.
+  C v[P::E];
+  fft_load<C, L, P>(v, tl, load);
+  load_twiddles<C, L>(tw, reinterpret_cast<const C*>(a.tw));
+  __syncthreads();
+  fft_run<C, S, L, NC, false, P>(sm, v, tw, col, tl, store);
 }
 
 struct RowArgs {
@@ -383,8 +387,6 @@ __global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NCM * Plan<L, V>::TPL)
   const int tid = threadIdx.x;
   const int tile = blockIdx.x;
   const int N = a.N;
-  load_twiddles<C, L>(tw, reinterpret_cast<const C*>(a.tw));
-  __syncthreads();
   {
     // column col = (mode pl, component c) with c fastest: one contiguous run
     const int col = tid % NC;
@@ -394,13 +396,15 @@ __global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NCM * Plan<L, V>::TPL)
     const bool valid = p < a.ninner;
     const C* Bp = reinterpret_cast<const C*>(a.B) + member * a.B_mem + (long long)tile * NC + col;
     const int B_row = int(a.B_row);  // L * B_row < 2^31, checked by the launcher
-    fft_columns<C, -1, L, SROW, true, P>(
-        sm, tw, col, tl,
-        [&](int m) -> C { return valid ? Bp[m * B_row] : cmk<C>(T(0), T(0)); },
-        [&](int m, C v) {
-          const int i = retained_row(m, N, L);
-          if (i >= 0) sm[i * SROW + col] = v;
-        });
+    // First-stage loads before the twiddle table, as in k_cols.
+    C v[P::E];
+    fft_load<C, L, P>(v, tl, [&](int m) -> C { return valid ? Bp[m * B_row] : cmk<C>(T(0), T(0)); });
+    load_twiddles<C, L>(tw, reinterpret_cast<const C*>(a.tw));
+    __syncthreads();
+    fft_run<C, -1, L, SROW, true, P>(sm, v, tw, col, tl, [&](int m, C x) {
+      const int i = retained_row(m, N, L);
+      if (i >= 0) sm[i * SROW + col] = x;
+    });
   }
   __syncthreads();
 

@@ -401,28 +401,32 @@ struct Engine {
   }
 };
 
-// Runs a full transform of the columns held by this CTA.
-//   load(row) -> C     gives the first-stage input at `row`
-//   store(row, C)      receives output bin `row`
-// SYNC_STORE: put a barrier before the stores (needed when they go to sm).
-// Threads with active == false take part in the barriers only: they neither
-// load, compute nor store.
-template <typename C, int S, int L, int SROW, bool SYNC_STORE, typename P = Plan<L>, typename Load,
-          typename Store>
-__device__ __forceinline__ void fft_columns(C* sm, const C* tw, int col, int tl, Load&& load,
-                                            Store&& store, bool active = true) {
+// The first stage's inputs of a thread: v[q R0 + r] = load(in_row(q, r)).
+// Split from the transform so a kernel can issue these loads before waiting
+// for its twiddle table.
+template <typename C, int L, typename P = Plan<L>, typename Load>
+__device__ __forceinline__ void fft_load(C (&v)[P::E], int tl, Load&& load, bool active = true) {
   using Info = RadixInfo<typename P::R>;
-  using Eng = Engine<C, S, L, P::E, SROW>;
-  C v[P::E];
-  if (active) {
+  using Eng = Engine<C, -1, L, P::E, 1>;
+  if (!active) return;
 #pragma unroll
-    for (int q = 0; q < P::E / Info::first; ++q) {
+  for (int q = 0; q < P::E / Info::first; ++q) {
 #pragma unroll
-      for (int r = 0; r < Info::first; ++r) {
-        v[q * Info::first + r] = load(Eng::template in_row<Info::first>(tl, q, r));
-      }
+    for (int r = 0; r < Info::first; ++r) {
+      v[q * Info::first + r] = load(Eng::template in_row<Info::first>(tl, q, r));
     }
   }
+}
+
+// Runs every stage on inputs already in v (from fft_load) and hands the
+// outputs to store(row, value).  SYNC_STORE: put a barrier before the stores
+// (needed when they go to sm).  Threads with active == false take part in
+// the barriers only: they neither load, compute nor store.
+template <typename C, int S, int L, int SROW, bool SYNC_STORE, typename P = Plan<L>, typename Store>
+__device__ __forceinline__ void fft_run(C* sm, C (&v)[P::E], const C* tw, int col, int tl, Store&& store,
+                                        bool active = true) {
+  using Info = RadixInfo<typename P::R>;
+  using Eng = Engine<C, S, L, P::E, SROW>;
   Eng::template run<1>(sm, v, col, tl, tw, active, typename P::R{});
   if constexpr (SYNC_STORE) __syncthreads();
   if (!active) return;
@@ -433,6 +437,18 @@ __device__ __forceinline__ void fft_columns(C* sm, const C* tw, int col, int tl,
       store(Eng::template out_row<Info::last>(tl, q, r), v[q * Info::last + r]);
     }
   }
+}
+
+// Runs a full transform of the columns held by this CTA.
+//   load(row) -> C     gives the first-stage input at `row`
+//   store(row, C)      receives output bin `row`
+template <typename C, int S, int L, int SROW, bool SYNC_STORE, typename P = Plan<L>, typename Load,
+          typename Store>
+__device__ __forceinline__ void fft_columns(C* sm, const C* tw, int col, int tl, Load&& load,
+                                            Store&& store, bool active = true) {
+  C v[P::E];
+  fft_load<C, L, P>(v, tl, load, active);
+  fft_run<C, S, L, SROW, SYNC_STORE, P>(sm, v, tw, col, tl, store, active);
 }
 
 // Copies the twiddle table W_L^m (m in [0,L)) from global into shared memory.
