@@ -369,8 +369,14 @@ template <typename T> __device__ __forceinline__ T visc_from_k2(const Visc& v, T
 //   MODE_RK2:  out = 3/4 u0 + 1/4 (u + dt dudt)       (ssp_rk3.hpp:57-58)
 //   MODE_RK3:  out = 2/3 (u + dt dudt) + 1/3 u0       (ssp_rk3.hpp:60-61)
 // grid = (ntile, nmembers); block = NB * NCM * L/E.
+// FP32 std plans: two resident CTAs per SM.
+template <typename T, int L, int NCM, int DIM, int V> struct EpiMinBlocks {
+  static constexpr int value = (sizeof(T) == 4 && V == 0) ? 2 : 1;
+};
+
 template <typename T, int L, int NCM, int DIM, int V>
-__global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NCM * Plan<L, V>::TPL)
+__global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NCM * Plan<L, V>::TPL,
+                                  EpiMinBlocks<T, L, NCM, DIM, V>::value)
     k_fwd_epilogue(EpiArgs a) {
   using C = cvec<T>;
   using P = Plan<L, V>;
@@ -431,16 +437,34 @@ __global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NCM * Plan<L, V>::TPL)
     k2 = twopi * T(j >= N / 2 + 1 ? j - N : j);
     k3 = twopi * T(kk);
   }
-  for (int i = tid / NCM; i < N; i += NT / NCM) {
+  // Rows of this thread: i = tid / NCM + it * ISTEP.  For the first MAXIT
+  // rows (all of them when N <= 2L/3 + 1, the 3/2 padding) its state values
+  // (u, and u0 for the RK2/RK3 combinations) are loaded first, so their
+  // latencies overlap; further rows load as they go.
+  constexpr int ISTEP = NT / NCM;
+  constexpr int MAXIT = (2 * L / 3 + 1 + ISTEP - 1) / ISTEP;
+  const int i0 = tid / NCM;
+  const bool need_u0 = a.mode == MODE_RK2 || a.mode == MODE_RK3;
+  C uv[MAXIT][DIM], wv[MAXIT][DIM];
+#pragma unroll
+  for (int it = 0; it < MAXIT; ++it) {
+    const int i = i0 + it * ISTEP;
+    if (i < N) {
+      const int off = i * u_row + p;
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) {
+        uv[it][c] = u[c * u_comp + off];
+        wv[it][c] = need_u0 ? u0[c * u_comp + off] : cmk<C>(T(0), T(0));
+      }
+    }
+  }
+  auto process = [&](int i, const C (&uc_)[DIM], const C (&wc_)[DIM]) {
+    const int off = i * u_row + p;
     const int i_ = i >= N / 2 + 1 ? i - N : i;
     const T k1 = twopi * T(i_);
     C Bv[NB];
 #pragma unroll
     for (int c = 0; c < NB; ++c) Bv[c] = sm[i * SROW + pl * NB + c];
-    const int off = i * u_row + p;
-    C uv[DIM];
-#pragma unroll
-    for (int c = 0; c < DIM; ++c) uv[c] = u[c * u_comp + off];
     // b = i k.B (force = 0), then L = b - k (k.b) / |k|^2
     C Lh[DIM];
     T absk2;
@@ -471,27 +495,40 @@ __global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NCM * Plan<L, V>::TPL)
     const bool zero = absk2 == T(0);
 #pragma unroll
     for (int c = 0; c < DIM; ++c) {
-      const C d = zero ? cmk<C>(T(0), T(0))
-                       : cmk<C>(-Lh[c].x + nu * uv[c].x, -Lh[c].y + nu * uv[c].y);
+      const C uc = uc_[c];
+      const C d = zero ? cmk<C>(T(0), T(0)) : cmk<C>(-Lh[c].x + nu * uc.x, -Lh[c].y + nu * uc.y);
       C r;
       if (a.mode == MODE_DUDT) {
         r = d;
       } else {
-        const C t = cmk<C>(uv[c].x + dt * d.x, uv[c].y + dt * d.y);
+        const C t = cmk<C>(uc.x + dt * d.x, uc.y + dt * d.y);
+        const C w = wc_[c];
         if (a.mode == MODE_RK1) {
           r = t;
+        } else if (a.mode == MODE_RK2) {
+          r = cmk<C>(T(0.75) * w.x + T(0.25) * t.x, T(0.75) * w.y + T(0.25) * t.y);
         } else {
-          const C w = u0[c * u_comp + off];
-          if (a.mode == MODE_RK2) {
-            r = cmk<C>(T(0.75) * w.x + T(0.25) * t.x, T(0.75) * w.y + T(0.25) * t.y);
-          } else {
-            const T c23 = T(2.0 / 3.0), c13 = T(1.0 / 3.0);
-            r = cmk<C>(c23 * t.x + c13 * w.x, c23 * t.y + c13 * w.y);
-          }
+          const T c23 = T(2.0 / 3.0), c13 = T(1.0 / 3.0);
+          r = cmk<C>(c23 * t.x + c13 * w.x, c23 * t.y + c13 * w.y);
         }
       }
       out[c * u_comp + off] = r;
     }
+  };
+#pragma unroll
+  for (int it = 0; it < MAXIT; ++it) {
+    const int i = i0 + it * ISTEP;
+    if (i < N) process(i, uv[it], wv[it]);
+  }
+  for (int i = i0 + MAXIT * ISTEP; i < N; i += ISTEP) {
+    const int off = i * u_row + p;
+    C uc[DIM], wc[DIM];
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+      uc[c] = u[c * u_comp + off];
+      wc[c] = need_u0 ? u0[c * u_comp + off] : cmk<C>(T(0), T(0));
+    }
+    process(i, uc, wc);
   }
 }
 
