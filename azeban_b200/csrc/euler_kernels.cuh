@@ -58,6 +58,7 @@ struct ColArgs {
   int clear_max;  // nonzero: also reset the member's CFL accumulator
   int in_ci;      // input component interleave: column p reads component p % in_ci
                   // at in_comp stride, position p / in_ci (1: plain columns)
+  long long nouter_tiles;  // outer slabs (k_cols2: tile space = ntile * nouter_tiles)
 };
 
 // Batched column transforms along a strided axis.  grid = (ntile * nouter,
@@ -112,6 +113,97 @@ __global__ void __launch_bounds__(NC * Plan<L, V>::TPL) k_cols(ColArgs a) {
   load_twiddles<C, L>(tw, reinterpret_cast<const C*>(a.tw));
   __syncthreads();
   fft_run<C, S, L, NC, false, P>(sm, v, tw, col, tl, store);
+}
+
+// Two-tile form of k_cols for plain (non-interleaved) inputs: a CTA takes
+// tiles 2 bx and 2 bx + 1 of the (tile, outer) space, starts cp.async copies
+// of both tiles' input rows into two shared buffers at once, transforms the
+// first in place while the second's copies are in flight, then the second.
+// Each thread copies its own column (col = tid % NC) on rows tid / NC + k L/E,
+// so a copy costs a pointer step and one cp.async.
+// grid = (ceil(ntile * nouter / 2), ncomp, nmembers); block = NC * L/E.
+template <int BYTES>
+__device__ __forceinline__ void cp_async_zfill(void* smem_dst, const void* gsrc, bool valid) {
+  const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  const int n = valid ? BYTES : 0;
+  if constexpr (BYTES == 16) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gsrc), "r"(n) : "memory");
+  } else {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gsrc), "r"(n) : "memory");
+  }
+}
+
+template <typename T, int L, int NC, int S, int MODE, int V>
+__global__ void __launch_bounds__(NC * Plan<L, V>::TPL) k_cols2(ColArgs a) {
+  using C = cvec<T>;
+  using P = Plan<L, V>;
+  constexpr int TPL = P::TPL;
+  extern __shared__ __align__(16) unsigned char az_smem[];
+  C* tw = reinterpret_cast<C*>(az_smem);
+  C* buf0 = tw + L;
+  const int member = blockIdx.z;
+  if (a.ctrl != nullptr) {
+    if (a.ctrl[member].skip) return;
+    if (a.clear_max && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
+      a.ctrl[member].umax64 = 0ull;
+      a.ctrl[member].umax32 = 0u;
+    }
+  }
+  const int col = threadIdx.x % NC;
+  const int tl = threadIdx.x / NC;
+  const int comp = blockIdx.y;
+  const int n = a.n_short;
+  const int in_rows = MODE == COL_PAD ? n : L;
+  const int in_row = int(a.in_row);
+  const int out_row = int(a.out_row);
+  const long long t0 = 2LL * blockIdx.x;
+  const long long tcount = (long long)a.ntile * a.nouter_tiles;
+  const int ntiles_here = t0 + 1 < tcount ? 2 : 1;
+  // Issue the copies of both tiles.
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    if (h < ntiles_here) {
+      const long long t = t0 + h;
+      const long long tile = t % a.ntile, outer = t / a.ntile;
+      const long long p = tile * NC + col;
+      const bool valid = p < a.ninner;
+      const C* src = reinterpret_cast<const C*>(a.in) + member * a.in_mem + outer * a.in_outer +
+                     comp * a.in_comp + (valid ? p : 0);
+      C* dst = buf0 + h * (L * NC) + col;
+      for (int r = tl; r < in_rows; r += TPL) cp_async_zfill<sizeof(C)>(dst + r * NC, src + r * in_row, valid);
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  }
+  load_twiddles<C, L>(tw, reinterpret_cast<const C*>(a.tw));
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    if (h == 0) {
+      asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+    } else {
+      asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    }
+    __syncthreads();
+    if (h < ntiles_here) {
+      const long long t = t0 + h;
+      const long long tile = t % a.ntile, outer = t / a.ntile;
+      const long long p = tile * NC + col;
+      const bool valid = p < a.ninner;
+      C* out = reinterpret_cast<C*>(a.out) + member * a.out_mem + comp * a.out_comp + outer * a.out_outer + p;
+      C* sm = buf0 + h * (L * NC);
+      fft_columns<C, S, L, NC, false, P>(
+          sm, tw, col, tl,
+          [&](int m) -> C {
+            int src = m;
+            if constexpr (MODE == COL_PAD) src = pad_src_row(m, n, L);
+            return src >= 0 ? sm[src * NC + col] : cmk<C>(T(0), T(0));
+          },
+          [&](int m, C v) {
+            int dst = m;
+            if constexpr (MODE == COL_TRUNC) dst = retained_row(m, n, L);
+            if (valid && dst >= 0) out[dst * out_row] = v;
+          });
+    }
+  }
 }
 
 struct RowArgs {

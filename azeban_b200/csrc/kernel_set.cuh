@@ -95,6 +95,31 @@ template <typename T, int L, int V> struct LaunchV {
     return (long long)L * a.in_row < lim && (long long)L * a.out_row < lim;
   }
 
+  // Two-tile kernel: g.x is the (tile, outer) count; each CTA takes two.
+  template <int S, int MODE>
+  static cudaError_t col2_kernel(const ColArgs& a, dim3 g, cudaStream_t st) {
+    constexpr int NC = TS::NC;
+    const size_t smem = size_t(L + 2 * L * NC) * sizeof(C);
+    auto k = k_cols2<T, L, NC, S, MODE, V>;
+    static const cudaError_t attr = set_smem(k, smem);
+    if (attr != cudaSuccess) return attr;
+    ColArgs b = a;
+    b.nouter_tiles = a.ntile > 0 ? (long long)g.x / a.ntile : 0;
+    const dim3 g2((g.x + 1) / 2, g.y, g.z);
+    k<<<g2, NC * TPL, smem, st>>>(b);
+    return cudaGetLastError();
+  }
+
+  static cudaError_t cols2(int kind, const ColArgs& a, dim3 g, cudaStream_t st) {
+    switch (kind) {
+      case COLK_PAD_INV: return col2_kernel<+1, COL_PAD>(a, g, st);
+      case COLK_PLAIN_INV: return col2_kernel<+1, COL_PLAIN>(a, g, st);
+      case COLK_TRUNC_FWD: return col2_kernel<-1, COL_TRUNC>(a, g, st);
+      case COLK_PLAIN_FWD: return col2_kernel<-1, COL_PLAIN>(a, g, st);
+      default: return cudaErrorInvalidValue;
+    }
+  }
+
   static cudaError_t cols(int kind, const ColArgs& a, dim3 g, cudaStream_t st) {
     if (!rows_fit(a)) return cudaErrorInvalidValue;
     switch (kind) {
@@ -206,7 +231,12 @@ template <typename T, int L> struct Launch {
   static cudaError_t cols(int v, int kind, const ColArgs& a, unsigned gx, unsigned gy, unsigned gz,
                           cudaStream_t st) {
     const dim3 g(gx, gy, gz);
-    return v ? LaunchV<T, L, 1>::cols(kind, a, g, st) : LaunchV<T, L, 0>::cols(kind, a, g, st);
+    // bit 1: the two-tile kernel, for plain (non-interleaved) inputs whose
+    // tile count divides evenly into the grid
+    if ((v & 2) && a.in_ci == 1 && a.ntile > 0 && gx % unsigned(a.ntile) == 0 &&
+        LaunchV<T, L, 0>::rows_fit(a))
+      return (v & 1) ? LaunchV<T, L, 1>::cols2(kind, a, g, st) : LaunchV<T, L, 0>::cols2(kind, a, g, st);
+    return (v & 1) ? LaunchV<T, L, 1>::cols(kind, a, g, st) : LaunchV<T, L, 0>::cols(kind, a, g, st);
   }
   static cudaError_t rows_product(int v, int dim, const RowArgs& a, unsigned gx, unsigned gy,
                                   cudaStream_t st) {

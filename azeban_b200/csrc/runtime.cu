@@ -59,7 +59,7 @@ int tuned_variant(int precision, int L, int kind) {
   if (const char* env = std::getenv("AZ_PLAN_VARIANT")) {
     int v[3] = {0, 0, 0};
     if (std::sscanf(env, "%d,%d,%d", &v[0], &v[1], &v[2]) == 3 && kind >= 0 && kind < 6)
-      return kind % 3 == 1 ? (v[1] & 3) : (v[kind % 3] & 1);
+      return kind % 3 == 2 ? (v[2] & 1) : (v[kind % 3] & 3);
   }
   return precision == 1 ? 1 : 0;
 }
@@ -341,7 +341,7 @@ static az_status rhs(az_euler e, const void* u, const void* u0, void* out, int m
   const KernelSet* ks = e->ks;
   const long long N = e->N, M = e->M, Nh = e->Nh;
   const unsigned B = unsigned(e->batch);
-  const int nc = ks->tiles[e->v_cols].nc;
+  const int nc = ks->tiles[e->v_cols & 1].nc;
   cudaError_t ce;
   if (e->dim == 3) {
     // pass 1: inverse along x with padding, state [3][N][N][Nh] -> A1 [M][N][Nh][3]
@@ -563,7 +563,7 @@ az_status az_euler_dt(az_euler e, double C, void* stream, double* out) {
 }
 
 az_status az_tune_set(int precision, int L, int kind, int variant) {
-  const int vmax = kind % 3 == 1 ? 3 : 1;
+  const int vmax = kind % 3 == 2 ? 1 : 3;
   if ((precision != 0 && precision != 1) || kind < 0 || kind > 5 || variant < 0 || variant > vmax)
     return fail(AZ_ERR_INVALID, "az_tune_set: bad argument");
   if (!kernel_set(precision, L)) return fail(AZ_ERR_UNSUPPORTED, "az_tune_set: no compiled length");
@@ -1169,7 +1169,7 @@ static az_status fft_axis(az_fft f, int ax, const void* in, void* out, int kind,
   c.out = out;
   c.tw = f->tw[ax];
   c.ninner = inner;
-  const int v = tuned_variant(f->prec, int(rows), 0);
+  const int v = tuned_variant(f->prec, int(rows), 0) & 1;  // plain FFT axes: plan bit only
   c.ntile = int(cdiv(inner, ks->tiles[v].nc));
   c.n_short = int(rows);
   c.in_row = inner;

@@ -30,14 +30,14 @@ KIND_PASSES = {0: (0, 1, 3), 1: (2,), 2: (4,)}  # pass ids per tuned kind (+3 fo
 VISC = {"type": "Smooth Cutoff", "eps": 0.05}
 
 
-# Kernel variants: bit 0 picks the radix plan (0 std, 1 wide); for the
-# contiguous-axis pass bit 1 picks the bulk-copy kernel.  The other kinds have
-# plan variants only.
+# Kernel variants: bit 0 picks the radix plan (0 std, 1 wide); bit 1 picks
+# the two-tile column kernel (column passes) or the bulk-copy kernel
+# (contiguous-axis pass).  The epilogue has plan variants only.
 RUNS = (0, 1, 2, 3)
 
 
 def _kind_variant(kind0: int, run: int) -> int:
-    return run if kind0 == 1 else run & 1
+    return run if kind0 in (0, 1) else run & 1
 
 
 def _set_all(prec: int, L: int, run: int) -> None:

@@ -200,10 +200,12 @@ size_t az_fft_work_area_size(az_fft fft);
  * kind: 0 column passes, 1 contiguous-axis passes, 2 epilogue pass of 3-D
  * solves (and of FFT<Dim>), 3-5 the same of 2-D solves.  Bit 0 picks the
  * radix plan (0: at most 24 elements per thread; 1: wide, fewer shared-memory
- * exchanges).  Contiguous-axis passes of solves (kinds 1, 4) also take bit 1,
- * the bulk-copy kernel (variants 0-3; plain FFT<Dim> row transforms use bit 0
- * only).  Other kinds: variants 0-1.
- * Applies to solves and FFTs created afterwards. */
+ * exchanges).  Bit 1: for column passes of solves (kinds 0, 3), the
+ * two-tile kernel that overlaps one tile's input copies with the other's
+ * transform; for contiguous-axis passes (kinds 1, 4), the bulk-copy kernel.
+ * Kinds 0, 1, 3, 4 take variants 0-3, the epilogue kinds 0-1 (plain FFT<Dim>
+ * transforms use bit 0 only).  Applies to solves and FFTs created
+ * afterwards. */
 az_status az_tune_set(int precision, int L, int kind, int variant);
 az_status az_tune_get(int precision, int L, int kind, int* variant);
 

@@ -1,8 +1,8 @@
 """Parity of every kernel variant of the right-hand side with the CPU oracle.
 
 The passes have several kernels: bit 0 of a variant picks the radix plan
-(0 std, 1 wide); for the contiguous-axis pass bit 1 picks the bulk-copy
-kernel.  The tuning table picks one per
+(0 std, 1 wide); bit 1 picks the two-tile column kernel for the column
+passes and the bulk-copy kernel for the contiguous-axis pass.  The tuning table picks one per
 (precision, length, kind); these tests pin each one against the oracle, so a
 table entry can never select a kernel whose results differ.  Tolerances as in
 test_gpu_euler.py.
@@ -50,7 +50,7 @@ class _Variants:
 
 @pytest.mark.parametrize("prec", ["f64", "f32"])
 @pytest.mark.parametrize("dim,N", [(2, 32), (2, 64), (2, 128), (3, 16), (3, 32)])
-@pytest.mark.parametrize("cols,rows,epi", [(0, 0, 0), (1, 1, 1), (0, 2, 0), (1, 3, 1), (1, 2, 0), (0, 3, 1)])
+@pytest.mark.parametrize("cols,rows,epi", [(0, 0, 0), (1, 1, 1), (0, 2, 0), (1, 3, 1), (2, 2, 0), (3, 3, 1)])
 def test_dudt_every_variant(prec, dim, N, cols, rows, epi):
     og = ora.Grid(dim, N)
     g = az.Grid(dim, N)
@@ -80,7 +80,7 @@ def test_bulk_copy_kernel_batch_members_match_single(prec, dim, N, B, rows):
     g = az.Grid(dim, N)
     v = az.make_viscosity(VISC_CFGS["smooth"], g)
     fields = [random_field_hat(dim, N, seed=900 + b) * (1.0 + 0.5 * b) for b in range(B)]
-    with _Variants(prec, g.N_phys_pad, dim, 0, rows, 0):
+    with _Variants(prec, g.N_phys_pad, dim, 2, rows, 0):
         eqB = az.IncompressibleEuler(g, v, prec, batch=B)
         simB = az.Simulation(g, 0.2, az.SSP_RK3(eqB), to_dev(np.stack(fields), prec))
         simB.simulate_until(0.02)
