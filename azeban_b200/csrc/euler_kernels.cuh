@@ -59,6 +59,11 @@ struct ColArgs {
   int in_ci;      // input component interleave: column p reads component p % in_ci
                   // at in_comp stride, position p / in_ci (1: plain columns)
   long long nouter_tiles;  // outer slabs (k_cols2: tile space = ntile * nouter_tiles)
+  // Grouped columns (grp > 0): column p is entry q = p % grp of group
+  // g = p / grp; entries q >= grp_valid are padding (not read, not written),
+  // and the input of entry q sits at g * in_grp + (q / in_ci or q).
+  int grp, grp_valid;
+  long long in_grp;
 };
 
 // Batched column transforms along a strided axis.  grid = (ntile * nouter,
@@ -86,8 +91,16 @@ __global__ void __launch_bounds__(NC * Plan<L, V>::TPL) k_cols(ColArgs a) {
   const int col = threadIdx.x % NC;
   const int tl = threadIdx.x / NC;
   const long long p = (long long)tile * NC + col;
-  const bool valid = p < a.ninner;
-  const long long pin = a.in_ci == 1 ? comp * a.in_comp + p : (p % a.in_ci) * a.in_comp + p / a.in_ci;
+  bool valid = p < a.ninner;
+  long long pin;
+  if (a.grp > 0) {
+    const long long g = p / a.grp;
+    const int q = int(p - g * a.grp);
+    valid = valid && q < a.grp_valid;
+    pin = g * a.in_grp + (a.in_ci == 1 ? comp * a.in_comp + q : (q % a.in_ci) * a.in_comp + q / a.in_ci);
+  } else {
+    pin = a.in_ci == 1 ? comp * a.in_comp + p : (p % a.in_ci) * a.in_comp + p / a.in_ci;
+  }
   const C* in = reinterpret_cast<const C*>(a.in) + member * a.in_mem + outer * a.in_outer + pin;
   C* out = reinterpret_cast<C*>(a.out) + member * a.out_mem + comp * a.out_comp +
            outer * a.out_outer + p;
@@ -418,6 +431,9 @@ struct EpiArgs {
   int mode;
   Visc visc;
   const Ctrl* ctrl;
+  // > 0: B's modes are grouped, nh per group with a group stride of b_grp
+  // elements (the padded rows of B2 [M][N][b_grp]); 0: contiguous modes.
+  long long b_grp;
 };
 
 // nu(|k|) of the reference's viscosity laws
@@ -492,7 +508,14 @@ __global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NCM * Plan<L, V>::TPL,
     const int pl = col / NB;
     const long long p = (long long)tile * NCM + pl;
     const bool valid = p < a.ninner;
-    const C* Bp = reinterpret_cast<const C*>(a.B) + member * a.B_mem + (long long)tile * NC + col;
+    long long bcol;
+    if (a.b_grp > 0) {
+      const long long g = p / a.nh;
+      bcol = g * a.b_grp + (p - g * a.nh) * NB + (col - pl * NB);
+    } else {
+      bcol = (long long)tile * NC + col;
+    }
+    const C* Bp = reinterpret_cast<const C*>(a.B) + member * a.B_mem + bcol;
     const int B_row = int(a.B_row);  // L * B_row < 2^31, checked by the launcher
     // First-stage loads before the twiddle table, as in k_cols.
     C v[P::E];

@@ -153,10 +153,11 @@ template <typename T, int L, int V> struct LaunchV {
     constexpr int NLP = ZTile<T, L, DIM, V>::NLP;
     using Z = ZShape<T, L, NLP, DIM, V>;
     auto k = k_zpass<T, L, NLP, DIM, V>;
-    const long long smem = Z::smem_bytes(a.nh);
+    const long long smem = Z::smem_bytes(a.in_line);
     if (smem < 0 || smem > 227 * 1024) return cudaErrorInvalidValue;
+    if (a.in_line < a.nh * DIM || a.out_line < a.nh * Z::NB) return cudaErrorInvalidValue;
     // The bulk copy needs a 16-byte aligned chunk of whole line pairs.
-    const long long lb = (long long)a.nh * DIM * Z::CB;
+    const long long lb = (long long)a.in_line * Z::CB;
     if ((reinterpret_cast<uintptr_t>(a.in) & 15) != 0 || (2 * lb) % 16 != 0 ||
         (a.in_mem * Z::CB) % 16 != 0 || (a.nlines & 1) != 0)
       return cudaErrorInvalidValue;
@@ -233,7 +234,7 @@ template <typename T, int L> struct Launch {
     const dim3 g(gx, gy, gz);
     // bit 1: the two-tile kernel, for plain (non-interleaved) inputs whose
     // tile count divides evenly into the grid
-    if ((v & 2) && a.in_ci == 1 && a.ntile > 0 && gx % unsigned(a.ntile) == 0 &&
+    if ((v & 2) && a.in_ci == 1 && a.grp == 0 && a.ntile > 0 && gx % unsigned(a.ntile) == 0 &&
         LaunchV<T, L, 0>::rows_fit(a))
       return (v & 1) ? LaunchV<T, L, 1>::cols2(kind, a, g, st) : LaunchV<T, L, 0>::cols2(kind, a, g, st);
     return (v & 1) ? LaunchV<T, L, 1>::cols(kind, a, g, st) : LaunchV<T, L, 0>::cols(kind, a, g, st);

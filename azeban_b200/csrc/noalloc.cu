@@ -98,22 +98,8 @@ az_status az_euler_dudt_noalloc(int dim, long long N_phys, long long N_phys_pad,
   e.v_cols = tuned_variant(precision, int(N_phys_pad), kbase + 0);
   e.v_rows = tuned_variant(precision, int(N_phys_pad), kbase + 1);
   e.v_epi = tuned_variant(precision, int(N_phys_pad), kbase + 2);
-  const long long N = e.N, M = e.M, Nh = e.Nh;
-  if (dim == 3) {
-    e.buf_mem[0] = 6 * M * N * Nh;
-    e.buf_mem[1] = 3 * M * M * Nh;
-    e.buf_mem[2] = 6 * M * M * Nh;
-    e.state_mem = 3 * N * N * Nh;
-    e.norm = 1.0 / (std::pow(std::sqrt((double)N), 3) * std::pow(std::sqrt((double)M), 3));
-    e.Md = (double)(M * M * M);
-  } else {
-    e.buf_mem[0] = 2 * M * Nh;
-    e.buf_mem[1] = 3 * M * Nh;
-    e.buf_mem[2] = 0;
-    e.state_mem = 2 * N * Nh;
-    e.norm = 1.0 / (std::pow(std::sqrt((double)N), 2) * std::pow(std::sqrt((double)M), 2));
-    e.Md = (double)(M * M);
-  }
+  const long long M = e.M;
+  euler_layout(&e);
   e.state_elems = e.state_mem;
 
   // Scratch layout: control block | twiddle table | buf0 | buf1 | buf2.

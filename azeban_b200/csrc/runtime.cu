@@ -3,6 +3,7 @@
 // and one simulate_until.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -200,6 +201,49 @@ az_status az_supported_lengths(int* out, int cap, int* n) {
   return AZ_OK;
 }
 
+namespace azb {
+// Elements per 128-byte line of the equation's complex type.
+static long long pad_line(long long elems, size_t csize) {
+  const long long q = 128 / (long long)csize;
+  return (elems + q - 1) / q * q;
+}
+
+void euler_layout(az_euler_s* e) {
+  const long long N = e->N, M = e->M, Nh = e->Nh;
+  // Which intermediates get padded rows (bits 0-3: A1, A2, B1, B2).  Padding
+  // pays where a column pass reads the rows (forward y reads B1: 128-byte
+  // aligned tiles) and costs where a pass streams whole lines or groups its
+  // columns (the product pass reads A2, the epilogue B2, inverse x writes
+  // A1), so only B1 is padded unless AZ_PAD_MASK says otherwise.
+  int mask = 0x4;
+  if (const char* env = std::getenv("AZ_PAD_MASK")) mask = std::atoi(env) & 0xf;
+  auto row = [&](long long elems, int bit) { return (mask >> bit) & 1 ? pad_line(elems, e->csize) : elems; };
+  if (e->dim == 3) {
+    e->ra1 = row(3 * Nh, 0);
+    e->ra2 = row(3 * Nh, 1);
+    e->rb1 = row(6 * Nh, 2);
+    e->rb2 = row(6 * Nh, 3);
+    e->buf_mem[0] = std::max(M * N * e->ra1, M * N * e->rb2);  // A1 [M][N][ra1], later B2 [M][N][rb2]
+    e->buf_mem[1] = M * M * e->ra2;                             // A2 [M][M][ra2]
+    e->buf_mem[2] = M * M * e->rb1;                             // B1 [M][M][rb1]
+    e->state_mem = 3 * N * N * Nh;
+    e->norm = 1.0 / (std::pow(std::sqrt((double)N), 3) * std::pow(std::sqrt((double)M), 3));
+    e->Md = (double)(M * M * M);
+  } else {
+    e->ra1 = row(2 * Nh, 0);
+    e->rb1 = row(3 * Nh, 2);
+    e->ra2 = e->ra1;
+    e->rb2 = e->rb1;
+    e->buf_mem[0] = M * e->ra1;  // A1 [M][ra1]
+    e->buf_mem[1] = M * e->rb1;  // B1 [M][rb1]
+    e->buf_mem[2] = 0;
+    e->state_mem = 2 * N * Nh;
+    e->norm = 1.0 / (std::pow(std::sqrt((double)N), 2) * std::pow(std::sqrt((double)M), 2));
+    e->Md = (double)(M * M);
+  }
+}
+}  // namespace azb
+
 az_status az_euler_create(const az_euler_desc* d, az_euler* out) {
   if (!d || !out) return fail(AZ_ERR_INVALID, "az_euler_create: null argument");
   *out = nullptr;
@@ -232,22 +276,7 @@ az_status az_euler_create(const az_euler_desc* d, az_euler* out) {
   e->v_cols = tuned_variant(e->prec, int(e->M), kbase + 0);
   e->v_rows = tuned_variant(e->prec, int(e->M), kbase + 1);
   e->v_epi = tuned_variant(e->prec, int(e->M), kbase + 2);
-  const long long N = e->N, M = e->M, Nh = e->Nh;
-  if (e->dim == 3) {
-    e->buf_mem[0] = 6 * M * N * Nh;  // A1 [M][N][Nh][3], later B2 [M][N][Nh][6]
-    e->buf_mem[1] = 3 * M * M * Nh;  // A2 [M][M][Nh][3]
-    e->buf_mem[2] = 6 * M * M * Nh;  // B1 [M][M][Nh][6]
-    e->state_mem = 3 * N * N * Nh;
-    e->norm = 1.0 / (std::pow(std::sqrt((double)N), 3) * std::pow(std::sqrt((double)M), 3));
-    e->Md = (double)(M * M * M);
-  } else {
-    e->buf_mem[0] = 2 * M * Nh;  // A1 [M][Nh][2]
-    e->buf_mem[1] = 3 * M * Nh;  // B1 [M][Nh][3]
-    e->buf_mem[2] = 0;
-    e->state_mem = 2 * N * Nh;
-    e->norm = 1.0 / (std::pow(std::sqrt((double)N), 2) * std::pow(std::sqrt((double)M), 2));
-    e->Md = (double)(M * M);
-  }
+  euler_layout(e);
   e->state_elems = e->state_mem * e->batch;
   size_t off[3];
   size_t total = 0;
@@ -256,7 +285,7 @@ az_status az_euler_create(const az_euler_desc* d, az_euler* out) {
     const size_t bytes = size_t(e->buf_mem[b]) * e->batch * e->csize;
     total += (bytes + 255) / 256 * 256;
   }
-  az_status st = twiddles(e->prec, int(M), &e->tw);
+  az_status st = twiddles(e->prec, int(e->M), &e->tw);
   if (st != AZ_OK) {
     delete e;
     return st;
@@ -324,6 +353,8 @@ static cudaError_t product_pass(az_euler e, int dim, const RowArgs& r, cudaStrea
     z.nlines = r.nlines;
     z.nh = r.nh;
     z.nmem = e->batch;
+    z.in_line = int(r.in_line);
+    z.out_line = int(r.out_line);
     z.in_mem = r.in_mem;
     z.out_mem = r.out_mem;
     z.norm = r.norm;
@@ -344,16 +375,22 @@ static az_status rhs(az_euler e, const void* u, const void* u0, void* out, int m
   const int nc = ks->tiles[e->v_cols & 1].nc;
   cudaError_t ce;
   if (e->dim == 3) {
-    // pass 1: inverse along x with padding, state [3][N][N][Nh] -> A1 [M][N][Nh][3]
+    // pass 1: inverse along x with padding, state [3][N][N][Nh] -> A1 [M][N][r3]
+    // (column p: group y = p / r3, entry q = 3 z + component, q < 3 Nh)
     ColArgs a1{};
     a1.in = u;
     a1.out = e->buf[0];
     a1.tw = e->tw;
-    a1.ninner = 3 * N * Nh;
+    a1.ninner = N * e->ra1;
     a1.ntile = int(cdiv(a1.ninner, nc));
     a1.n_short = int(N);
     a1.in_row = N * Nh;
-    a1.out_row = 3 * N * Nh;
+    a1.out_row = N * e->ra1;
+    if (e->ra1 != 3 * Nh) {
+      a1.grp = int(e->ra1);
+      a1.grp_valid = int(3 * Nh);
+      a1.in_grp = Nh;
+    }
     a1.in_comp = N * N * Nh;
     a1.in_ci = 3;
     a1.in_mem = e->state_mem;
@@ -365,7 +402,7 @@ static az_status rhs(az_euler e, const void* u, const void* u0, void* out, int m
       ce = ks->cols(e->v_cols, COLK_PAD_INV, a1, unsigned(a1.ntile), 1, B, st);
     }
     if (ce != cudaSuccess) return cuda_fail(ce, "rhs pass 1");
-    // pass 2: inverse along y with padding, A1 -> A2 [M][M][Nh][3]
+    // pass 2: inverse along y with padding, A1 -> A2 [M][M][r3]
     ColArgs a2{};
     a2.in = e->buf[0];
     a2.out = e->buf[1];
@@ -373,10 +410,10 @@ static az_status rhs(az_euler e, const void* u, const void* u0, void* out, int m
     a2.ninner = 3 * Nh;
     a2.ntile = int(cdiv(a2.ninner, nc));
     a2.n_short = int(N);
-    a2.in_row = 3 * Nh;
-    a2.out_row = 3 * Nh;
-    a2.in_outer = N * 3 * Nh;
-    a2.out_outer = M * 3 * Nh;
+    a2.in_row = e->ra1;
+    a2.out_row = e->ra2;
+    a2.in_outer = N * e->ra1;
+    a2.out_outer = M * e->ra2;
     a2.in_ci = 1;
     a2.in_mem = e->buf_mem[0];
     a2.out_mem = e->buf_mem[1];
@@ -386,15 +423,15 @@ static az_status rhs(az_euler e, const void* u, const void* u0, void* out, int m
       ce = ks->cols(e->v_cols, COLK_PAD_INV, a2, unsigned(a2.ntile * M), 1, B, st);
     }
     if (ce != cudaSuccess) return cuda_fail(ce, "rhs pass 2");
-    // pass 3: z lines, product, CFL max: A2 -> B1 [M][M][Nh][6]
+    // pass 3: z lines, product, CFL max: A2 -> B1 [M][M][r6]
     RowArgs r{};
     r.in = e->buf[1];
     r.out = e->buf[2];
     r.tw = e->tw;
     r.nlines = M * M;
     r.nh = int(Nh);
-    r.in_line = 3 * Nh;
-    r.out_line = 6 * Nh;
+    r.in_line = e->ra2;
+    r.out_line = e->rb1;
     r.in_mem = e->buf_mem[1];
     r.out_mem = e->buf_mem[2];
     r.norm = e->norm;
@@ -405,7 +442,7 @@ static az_status rhs(az_euler e, const void* u, const void* u0, void* out, int m
     }
     if (ce != cudaSuccess) return cuda_fail(ce, "rhs pass 3");
   } else {
-    // pass 1: inverse along x with padding, state [2][N][Nh] -> A1 [M][Nh][2]
+    // pass 1: inverse along x with padding, state [2][N][Nh] -> A1 [M][r3]
     ColArgs a1{};
     a1.in = u;
     a1.out = e->buf[0];
@@ -414,7 +451,7 @@ static az_status rhs(az_euler e, const void* u, const void* u0, void* out, int m
     a1.ntile = int(cdiv(a1.ninner, nc));
     a1.n_short = int(N);
     a1.in_row = Nh;
-    a1.out_row = 2 * Nh;
+    a1.out_row = e->ra1;
     a1.in_comp = N * Nh;
     a1.in_ci = 2;
     a1.in_mem = e->state_mem;
@@ -426,15 +463,15 @@ static az_status rhs(az_euler e, const void* u, const void* u0, void* out, int m
       ce = ks->cols(e->v_cols, COLK_PAD_INV, a1, unsigned(a1.ntile), 1, B, st);
     }
     if (ce != cudaSuccess) return cuda_fail(ce, "rhs pass 1 (2-D)");
-    // pass 2: y lines, product, CFL max: A1 -> B1 [M][Nh][3]
+    // pass 2: y lines, product, CFL max: A1 -> B1 [M][r6]
     RowArgs r{};
     r.in = e->buf[0];
     r.out = e->buf[1];
     r.tw = e->tw;
     r.nlines = M;
     r.nh = int(Nh);
-    r.in_line = 2 * Nh;
-    r.out_line = 3 * Nh;
+    r.in_line = e->ra1;
+    r.out_line = e->rb1;
     r.in_mem = e->buf_mem[0];
     r.out_mem = e->buf_mem[1];
     r.norm = e->norm;
@@ -453,7 +490,7 @@ static az_status rhs(az_euler e, const void* u, const void* u0, void* out, int m
   const char* bsrc;
   long long b_row, b_mem, ninner;
   if (e->dim == 3) {
-    // pass 4: forward along y, keep retained rows: B1 -> B2 [M][N][Nh][6]
+    // pass 4: forward along y, keep retained rows: B1 -> B2 [M][N][r6]
     ColArgs a4{};
     a4.in = e->buf[2];
     a4.out = e->buf[0];
@@ -461,10 +498,10 @@ static az_status rhs(az_euler e, const void* u, const void* u0, void* out, int m
     a4.ninner = 6 * Nh;
     a4.ntile = int(cdiv(a4.ninner, nc));
     a4.n_short = int(N);
-    a4.in_row = 6 * Nh;
-    a4.out_row = 6 * Nh;
-    a4.in_outer = M * 6 * Nh;
-    a4.out_outer = N * 6 * Nh;
+    a4.in_row = e->rb1;
+    a4.out_row = e->rb2;
+    a4.in_outer = M * e->rb1;
+    a4.out_outer = N * e->rb2;
     a4.in_ci = 1;
     a4.in_mem = e->buf_mem[2];
     a4.out_mem = e->buf_mem[0];
@@ -475,12 +512,12 @@ static az_status rhs(az_euler e, const void* u, const void* u0, void* out, int m
     }
     if (ce != cudaSuccess) return cuda_fail(ce, "rhs pass 4");
     bsrc = e->buf[0];
-    b_row = 6 * N * Nh;
+    b_row = N * e->rb2;
     b_mem = e->buf_mem[0];
     ninner = N * Nh;
   } else {
     bsrc = e->buf[1];
-    b_row = 3 * Nh;
+    b_row = e->rb1;
     b_mem = e->buf_mem[1];
     ninner = Nh;
   }
@@ -497,6 +534,7 @@ static az_status rhs(az_euler e, const void* u, const void* u0, void* out, int m
   ep.nh = int(Nh);
   ep.B_row = b_row;
   ep.B_mem = b_mem;
+  ep.b_grp = (e->dim == 3 && e->rb2 != 6 * Nh) ? e->rb2 : 0;
   ep.u_row = e->dim == 3 ? N * Nh : Nh;
   ep.u_comp = e->dim == 3 ? N * N * Nh : N * Nh;
   ep.u_mem = e->state_mem;

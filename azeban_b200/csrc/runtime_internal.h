@@ -21,6 +21,10 @@ struct az_euler_s {
   size_t work_bytes = 0;
   char* buf[3] = {nullptr, nullptr, nullptr};
   long long buf_mem[3] = {0, 0, 0};  // member strides (elements)
+  // Row strides (elements) of the intermediates; a padded one is a whole
+  // number of 128-byte lines.  3-D: A1, A2 rows of 3 Nh, B1, B2 rows of
+  // 6 Nh; 2-D: A1 rows of 2 Nh (ra1), B1 rows of 3 Nh (rb1).
+  long long ra1 = 0, ra2 = 0, rb1 = 0, rb2 = 0;
   long long state_mem;               // member stride of a state array
   long long state_elems;             // batch * state_mem
   azb::Ctrl* ctrl = nullptr;              // [batch]
@@ -36,6 +40,9 @@ constexpr int kDiagDoublesPerMember = 512 * 2 + 2;
 
 
 namespace azb {
+// Sizes, member strides, padded row strides, normalisation and M^d of an
+// equation whose dim, N, M, Nh and csize are set.
+void euler_layout(az_euler_s* e);
 // One right-hand side of every member of `e` (MODE_DUDT), the launch sequence
 // of az_euler_dudt: resets the members' skip flags, then runs the passes.
 az_status euler_dudt_launch(az_euler e, void* dudt_hat, const void* u_hat, cudaStream_t st);

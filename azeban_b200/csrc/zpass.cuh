@@ -67,12 +67,13 @@ template <typename T> constexpr T kFiniteMax = sizeof(T) == 4 ? T(3.402823466385
                                                                : T(1.79769313486231570814527423731704357e308);
 
 struct ZArgs {
-  const void* in;   // lines of nh x DIM complex, component innermost, contiguous
-  void* out;        // lines of nh x NB complex, component innermost
+  const void* in;   // lines of nh x DIM complex, component innermost, in_line apart
+  void* out;        // lines of nh x NB complex, component innermost, out_line apart
   const void* tw;
   long long nlines;  // lines per member (even)
   int nh;            // spectral bins per line
   int nmem;          // members
+  int in_line, out_line;  // line strides (elements; multiples of 2 lines' 16 bytes)
   long long in_mem, out_mem;  // member strides (elements)
   double norm;       // 1 / (N^{d/2} M^{d/2})
   Ctrl* ctrl;
@@ -113,12 +114,12 @@ template <typename T, int L, int NLP, int DIM, int V> struct ZShape {
   static constexpr int OFF_V = REGIONS ? OFF_P + P_BYTES : OFF_P + VOFF * CB;
   static constexpr int OFF_IN = REGIONS ? OFF_P : OFF_P + P_BYTES;
   static constexpr int BYTES = REGIONS ? OFF_V + L * SV * CB : OFF_IN;
-  // complex elements of one chunk's input
-  static __host__ __device__ long long chunk_elems(int nh) { return 2LL * NLP * nh * DIM; }
+  // complex elements of one chunk's input (2 NLP lines of in_line)
+  static __host__ __device__ long long chunk_elems(int in_line) { return 2LL * NLP * in_line; }
   // -1 when the input does not fit in P (REGIONS), which holds it
-  static __host__ __device__ long long smem_bytes(int nh) {
-    if (REGIONS) return chunk_elems(nh) <= (long long)L * SP ? BYTES : -1;
-    return BYTES + chunk_elems(nh) * CB;
+  static __host__ __device__ long long smem_bytes(int in_line) {
+    if (REGIONS) return chunk_elems(in_line) <= (long long)L * SP ? BYTES : -1;
+    return BYTES + chunk_elems(in_line) * CB;
   }
 };
 
@@ -154,8 +155,8 @@ __global__ void __launch_bounds__(ZShape<T, L, NLP, DIM, V>::NT, ZShape<T, L, NL
   if (ctrl->skip) return;
   const int tid = threadIdx.x;
   const int nh = a.nh;
-  const int in_line = nh * DIM;
-  const int out_line = nh * NB;
+  const int in_line = a.in_line;
+  const int out_line = a.out_line;
   const long long line0 = (long long)blockIdx.x * 2 * NLP;
   // Line pairs of this chunk that exist (nlines is even, so a pair is whole).
   const int npairs = int((a.nlines - line0) / 2 < NLP ? (a.nlines - line0) / 2 : NLP);

@@ -92,3 +92,24 @@ def test_bulk_copy_kernel_batch_members_match_single(prec, dim, N, B, rows):
             sim1.simulate_until(0.02)
             assert sim1.state()[1][0] == nB[b]
             np.testing.assert_array_equal(to_host(sim1.u()), outB[b])
+
+
+@pytest.mark.parametrize("mask", [0, 5, 10, 15])
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("dim,N", [(2, 64), (3, 16), (3, 32)])
+def test_dudt_every_row_padding(mask, prec, dim, N, monkeypatch):
+    """The intermediates' rows may be padded to whole 128-byte lines
+    (AZ_PAD_MASK bits: A1, A2, B1, B2); every combination gives the oracle's
+    right-hand side, including the grouped column paths of the inverse x pass
+    and the epilogue."""
+    monkeypatch.setenv("AZ_PAD_MASK", str(mask))
+    og = ora.Grid(dim, N)
+    g = az.Grid(dim, N)
+    oeq = ora.IncompressibleEuler(og, ora.make_viscosity(VISC_CFGS["smooth"], og))
+    u_hat = random_field_hat(dim, N, seed=500 + N)
+    ref = oeq.dudt(u_hat)
+    eq = az.IncompressibleEuler(g, az.make_viscosity(VISC_CFGS["smooth"], g), prec)
+    d_u = to_dev(u_hat, prec)
+    d_out = torch.empty_like(d_u)
+    eq.dudt(d_out, d_u)
+    assert rel_l2(to_host(d_out), ref) <= TOL[prec]
