@@ -195,16 +195,12 @@ def run_ours(args, rank, world, local):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
 
-    def barrier():
-        if dist is not None:
-            dist.barrier()
+    from azeban_b200 import replicas
+
+    barrier = replicas.barrier
 
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.max_over_ranks(x)
 
     N, B, K, W = args.n, args.batch, args.steps, args.warmup
     g = az.Grid(3, N)
@@ -235,7 +231,7 @@ def run_ours(args, rank, world, local):
     barrier()
     step_ms = [evs[i].elapsed_time(evs[i + 1]) for i in range(K)]
     total_ms = max_over_ranks(evs[0].elapsed_time(evs[K]))
-    value = world * B * K / (total_ms / 1e3)
+    value = replicas.aggregate_rate(B * K, world, total_ms)
     ms_per_step = total_ms / K
     sorted_ms = sorted(step_ms)
     p50 = sorted_ms[len(sorted_ms) // 2]
