@@ -62,9 +62,25 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned b
       : "memory");
 }
 
-// Largest finite value: |x| <= kFiniteMax is false exactly for inf and NaN.
-template <typename T> constexpr T kFiniteMax = sizeof(T) == 4 ? T(3.40282346638528859811704183484516925e38)
-                                                               : T(1.79769313486231570814527423731704357e308);
+// |x| as its IEEE bit pattern with the sign cleared.  For such patterns the
+// unsigned order is the order of the values, and infinity and every NaN sort
+// above all finite values, so one unsigned max gives max |x| and tells
+// whether a non-finite value was met (the result is >= kInfBits).
+template <typename T> struct AbsBits;
+template <> struct AbsBits<float> {
+  using U = unsigned int;
+  static constexpr U kInfBits = 0x7f800000u;
+  static __device__ __forceinline__ U of(float x) { return __float_as_uint(x) & 0x7fffffffu; }
+  static __device__ __forceinline__ void to_ctrl(Ctrl* c, U b) { atomicMax(&c->umax32, b); }
+};
+template <> struct AbsBits<double> {
+  using U = unsigned long long;
+  static constexpr U kInfBits = 0x7ff0000000000000ull;
+  static __device__ __forceinline__ U of(double x) {
+    return static_cast<U>(__double_as_longlong(x)) & 0x7fffffffffffffffull;
+  }
+  static __device__ __forceinline__ void to_ctrl(Ctrl* c, U b) { atomicMax(&c->umax64, b); }
+};
 
 struct ZArgs {
   const void* in;   // lines of nh x DIM complex, component innermost, in_line apart
@@ -177,8 +193,8 @@ __global__ void __launch_bounds__(ZShape<T, L, NLP, DIM, V>::NT, ZShape<T, L, NL
     if (tid == 0) atomicOr(&ctrl->err, 2);
     return;
   }
-  T vmax = T(0);
-  bool bad = false;
+  using AB = AbsBits<T>;
+  typename AB::U vbits = 0;  // running max |u| as bits (see AbsBits)
 
   // 1. Hermitian extension into V: column (pair p, slot q) holds signal 2q +
   //    i * signal 2q+1, signal s = component s % DIM of line s / DIM of the
@@ -242,9 +258,8 @@ __global__ void __launch_bounds__(ZShape<T, L, NLP, DIM, V>::NT, ZShape<T, L, NL
     }
 #pragma unroll
     for (int s = 0; s < 2 * DIM; ++s) {
-      const T av = fabs(u[s]);
-      bad |= !(av <= kFiniteMax<T>);
-      vmax = fmax(vmax, av);
+      const typename AB::U b = AB::of(u[s]);
+      vbits = b > vbits ? b : vbits;
       u[s] *= norm;
     }
     C* w = pw + m * SP + p * NB;
@@ -299,25 +314,25 @@ __global__ void __launch_bounds__(ZShape<T, L, NLP, DIM, V>::NT, ZShape<T, L, NL
     }
   }
 
-  // CFL reduction: warp, then block, then one atomic per CTA.
+  // CFL reduction: warp, then block, then one atomic per CTA.  A non-finite
+  // value sets the error bit; the maximum then records infinity.
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) vmax = fmax(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
-  const unsigned anybad = __any_sync(0xffffffffu, bad);
-  __shared__ T red[NT / 32];
-  __shared__ int redbad;
-  if (tid == 0) redbad = 0;
-  __syncthreads();
-  if ((tid & 31) == 0) {
-    red[tid >> 5] = vmax;
-    if (anybad) redbad = 1;
+  for (int o = 16; o > 0; o >>= 1) {
+    const typename AB::U other = __shfl_xor_sync(0xffffffffu, vbits, o);
+    vbits = other > vbits ? other : vbits;
   }
+  __shared__ typename AB::U red[NT / 32];
+  if ((tid & 31) == 0) red[tid >> 5] = vbits;
   __syncthreads();
   if (tid == 0) {
-    T m = T(0);
+    typename AB::U m = 0;
 #pragma unroll
-    for (int w = 0; w < NT / 32; ++w) m = fmax(m, red[w]);
-    atomic_max_abs<T>(ctrl, m);
-    if (redbad) atomicOr(&ctrl->err, 1);
+    for (int w = 0; w < NT / 32; ++w) m = red[w] > m ? red[w] : m;
+    if (m >= AB::kInfBits) {
+      atomicOr(&ctrl->err, 1);
+      m = AB::kInfBits;
+    }
+    AB::to_ctrl(ctrl, m);
   }
 }
 
