@@ -5,8 +5,8 @@
 // products, bins [0, nh) kept), but the input of a CTA's chunk of 2 NLP lines
 // is one contiguous run of global memory, so a single elected thread moves it
 // into shared memory with one cp.async.bulk, completing on an mbarrier: no
-// thread issues a global load, and the phases that follow index shared memory
-// with plain row/column arithmetic instead of a Hermitian-extension gather.
+// thread issues a global load.  The inverse transform's first stage reads the
+// half spectra there directly, the Hermitian extension folded into its loads.
 // The mbarrier wait is bounded; a wait that runs out sets bit 1 of the
 // member's error word and the CTA returns.
 //
@@ -62,6 +62,16 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned b
       : "memory");
 }
 
+// Two adjacent complex elements: one 16-byte store for FP32, else two.
+template <typename C> __device__ __forceinline__ void store2(C* dst, C a, C b) {
+  if constexpr (sizeof(C) == 8) {
+    *reinterpret_cast<float4*>(dst) = make_float4(a.x, a.y, b.x, b.y);
+  } else {
+    dst[0] = a;
+    dst[1] = b;
+  }
+}
+
 // |x| as its IEEE bit pattern with the sign cleared.  For such patterns the
 // unsigned order is the order of the values, and infinity and every NaN sort
 // above all finite values, so one unsigned max gives max |x| and tells
@@ -112,6 +122,10 @@ struct ZArgs {
 template <typename T, int L, int NLP, int DIM, int V> struct ZShape {
   static constexpr int CB = int(sizeof(cvec<T>));
   static constexpr bool REGIONS = CB == 8;
+  // FP32 with an even number of products: the products go to P as 16-byte
+  // pairs (with rows of 24 elements a quarter-warp's stores then fall on
+  // distinct bank groups)
+  static constexpr bool PAIRED = REGIONS && (DIM * (DIM + 1) / 2) % 2 == 0;
   static constexpr int NB = DIM * (DIM + 1) / 2;
   static constexpr int NINV = DIM * NLP;
   static constexpr int NFWD = NB * NLP;
@@ -196,52 +210,42 @@ __global__ void __launch_bounds__(ZShape<T, L, NLP, DIM, V>::NT, ZShape<T, L, NL
   using AB = AbsBits<T>;
   typename AB::U vbits = 0;  // running max |u| as bits (see AbsBits)
 
-  // 1. Hermitian extension into V: column (pair p, slot q) holds signal 2q +
-  //    i * signal 2q+1, signal s = component s % DIM of line s / DIM of the
-  //    pair.  Bin k < nh gives rows k and L - k; rows [nh, L - nh] are zero.
-  //    The imaginary parts of bin 0 and bin L/2 are dropped, as a c2r does.
-  //    REGIONS: lanes run over pairs fastest, then bins; else over bins.
-  for (int idx = tid; idx < NLP * nh; idx += NT) {
-    const int kb = Z::REGIONS ? idx / NLP : idx % nh;
-    const int p = Z::REGIONS ? idx % NLP : idx / nh;
-    C sg[2 * DIM];
-    const C* src = cin + (2 * p) * in_line + kb * DIM;
-#pragma unroll
-    for (int s = 0; s < 2 * DIM; ++s)
-      sg[s] = p < npairs ? src[(s / DIM) * in_line + s % DIM] : cmk<C>(T(0), T(0));
-    const bool edge = kb == 0 || 2 * kb == L;
-    if (edge) {
-#pragma unroll
-      for (int s = 0; s < 2 * DIM; ++s) sg[s].y = T(0);
-    }
-    C* row = vw + kb * SV + p * DIM;
-    C* mrow = vw + (L - kb) * SV + p * DIM;
-#pragma unroll
-    for (int q = 0; q < DIM; ++q) {
-      const C x = sg[2 * q], y = sg[2 * q + 1];
-      row[q] = cmk<C>(x.x - y.y, x.y + y.x);
-      if (!edge) mrow[q] = cmk<C>(x.x + y.y, y.x - x.y);
-    }
-  }
-  for (int idx = tid; idx < (L - 2 * nh + 1) * NINV; idx += NT) {
-    const int r = idx / NINV;
-    vw[(nh + r) * SV + (idx - r * NINV)] = cmk<C>(T(0), T(0));
-  }
-  __syncthreads();
-
-  // 2. Inverse transforms of the velocity columns, in place in V.
+  // 1. Inverse transforms of the velocity columns into V.  Column (pair p,
+  //    component q) holds component q of line 2p + i * component q of line
+  //    2p+1.  Its first-stage inputs come straight from the chunk's half
+  //    spectra: bin k < nh gives row k (X + iY) and row L - k (conj X + i
+  //    conj Y); rows [nh, L - nh] are zero.  The imaginary parts of bin 0
+  //    and bin L/2 are dropped, as a c2r does.
   {
     using PI = typename InvPlan<L, V, NINV, NT>::type;
     const bool active = tid < NINV * PI::TPL;
     const int col = active ? tid % NINV : 0;
     const int tl = active ? tid / NINV : 0;
+    const int p = col / DIM;
+    const C* la = cin + (2 * p) * in_line + (col - p * DIM);
+    const C* lb = la + in_line;
+    const bool live = p < npairs;
+    auto load = [&](int m) {
+      const bool lo = m < nh;
+      const bool hi = m > L - nh;
+      const int k = lo ? m : L - m;
+      C x = cmk<C>(T(0), T(0)), y = x;
+      if (live && (lo || hi)) {
+        x = la[k * DIM];
+        y = lb[k * DIM];
+      }
+      if (m == 0 || 2 * m == L) {
+        x.y = T(0);
+        y.y = T(0);
+      }
+      return lo ? cmk<C>(x.x - y.y, x.y + y.x) : cmk<C>(x.x + y.y, y.x - x.y);
+    };
     fft_columns<C, +1, L, SV, true, PI>(
-        vw, tw, col, tl, [&](int m) { return vw[m * SV + col]; },
-        [&](int m, C v) { vw[m * SV + col] = v; }, active);
+        vw, tw, col, tl, load, [&](int m, C v) { vw[m * SV + col] = v; }, active);
   }
   __syncthreads();
 
-  // 3. CFL maximum and products B = u (x) u in the reference's component
+  // 2. CFL maximum and products B = u (x) u in the reference's component
   //    order (product c of line a in the real part, of line b in the
   //    imaginary part), from V into P.  REGIONS: lanes run over pairs
   //    fastest.  Else a thread owns a row and handles its pairs in order
@@ -253,8 +257,8 @@ __global__ void __launch_bounds__(ZShape<T, L, NLP, DIM, V>::NT, ZShape<T, L, NL
 #pragma unroll
     for (int q = 0; q < DIM; ++q) {
       const C z = v[q];
-      u[2 * q] = z.x;
-      u[2 * q + 1] = z.y;
+      u[q] = z.x;        // line a
+      u[DIM + q] = z.y;  // line b
     }
 #pragma unroll
     for (int s = 0; s < 2 * DIM; ++s) {
@@ -267,6 +271,10 @@ __global__ void __launch_bounds__(ZShape<T, L, NLP, DIM, V>::NT, ZShape<T, L, NL
       w[0] = cmk<C>(u[0] * u[0], u[2] * u[2]);
       w[1] = cmk<C>(u[0] * u[1], u[2] * u[3]);
       w[2] = cmk<C>(u[1] * u[1], u[3] * u[3]);
+    } else if constexpr (Z::PAIRED) {
+      store2(w, cmk<C>(u[0] * u[0], u[3] * u[3]), cmk<C>(u[1] * u[0], u[4] * u[3]));
+      store2(w + 2, cmk<C>(u[1] * u[1], u[4] * u[4]), cmk<C>(u[2] * u[0], u[5] * u[3]));
+      store2(w + 4, cmk<C>(u[2] * u[1], u[5] * u[4]), cmk<C>(u[2] * u[2], u[5] * u[5]));
     } else {
       w[0] = cmk<C>(u[0] * u[0], u[3] * u[3]);
       w[1] = cmk<C>(u[1] * u[0], u[4] * u[3]);
@@ -286,7 +294,7 @@ __global__ void __launch_bounds__(ZShape<T, L, NLP, DIM, V>::NT, ZShape<T, L, NL
   }
   __syncthreads();
 
-  // 4. Forward transforms of the NFWD product columns, in place in P.
+  // 3. Forward transforms of the NFWD product columns, in place in P.
   {
     const int col = tid % NFWD;
     const int tl = tid / NFWD;
@@ -296,7 +304,7 @@ __global__ void __launch_bounds__(ZShape<T, L, NLP, DIM, V>::NT, ZShape<T, L, NL
   }
   __syncthreads();
 
-  // 5. Separate the two real spectra and write bins [0, nh), component
+  // 4. Separate the two real spectra and write bins [0, nh), component
   //    fastest, so consecutive threads store consecutive elements of a line.
   C* out = reinterpret_cast<C*>(a.out) + member * a.out_mem + line0 * out_line;
   const int nb_nh = NB * nh;
