@@ -537,6 +537,12 @@ __global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NCM * Plan<L, V>::TPL,
   C* out = reinterpret_cast<C*>(a.out) + member * a.u_mem;
   const int u_row = int(a.u_row), u_comp = int(a.u_comp);  // a member's state < 2^31 elements
   const T inv_k0sq = T(1.0 / (a.visc.k0 * a.visc.k0));
+  // The stage combination as uniform coefficients instead of per-element
+  // branches: t = u + dt d (d itself for MODE_DUDT), r = ct t + cw u0.
+  const bool use_u = a.mode != MODE_DUDT;
+  const T dd = use_u ? dt : T(1);
+  const T ct = a.mode == MODE_RK2 ? T(0.25) : a.mode == MODE_RK3 ? T(2.0 / 3.0) : T(1);
+  const T cw = a.mode == MODE_RK2 ? T(0.75) : a.mode == MODE_RK3 ? T(1.0 / 3.0) : T(0);
   // NT is a multiple of NCM, so a thread keeps one mode column pl (and its
   // second and third wavenumbers) and walks the retained rows i.
   const int pl = tid % NCM;
@@ -578,8 +584,20 @@ __global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NCM * Plan<L, V>::TPL,
     const int i_ = i >= N / 2 + 1 ? i - N : i;
     const T k1 = twopi * T(i_);
     C Bv[NB];
+    if constexpr (sizeof(C) == 8 && NB % 2 == 0) {
+      // 16-byte reads: with rows of NB * NCM elements a quarter-warp's reads
+      // fall on distinct bank groups
+      const float4* b4 = reinterpret_cast<const float4*>(sm + i * SROW + pl * NB);
 #pragma unroll
-    for (int c = 0; c < NB; ++c) Bv[c] = sm[i * SROW + pl * NB + c];
+      for (int c = 0; c < NB / 2; ++c) {
+        const float4 q = b4[c];
+        Bv[2 * c] = cmk<C>(q.x, q.y);
+        Bv[2 * c + 1] = cmk<C>(q.z, q.w);
+      }
+    } else {
+#pragma unroll
+      for (int c = 0; c < NB; ++c) Bv[c] = sm[i * SROW + pl * NB + c];
+    }
     // b = i k.B (force = 0), then L = b - k (k.b) / |k|^2
     C Lh[DIM];
     T absk2;
@@ -612,22 +630,9 @@ __global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NCM * Plan<L, V>::TPL,
     for (int c = 0; c < DIM; ++c) {
       const C uc = uc_[c];
       const C d = zero ? cmk<C>(T(0), T(0)) : cmk<C>(-Lh[c].x + nu * uc.x, -Lh[c].y + nu * uc.y);
-      C r;
-      if (a.mode == MODE_DUDT) {
-        r = d;
-      } else {
-        const C t = cmk<C>(uc.x + dt * d.x, uc.y + dt * d.y);
-        const C w = wc_[c];
-        if (a.mode == MODE_RK1) {
-          r = t;
-        } else if (a.mode == MODE_RK2) {
-          r = cmk<C>(T(0.75) * w.x + T(0.25) * t.x, T(0.75) * w.y + T(0.25) * t.y);
-        } else {
-          const T c23 = T(2.0 / 3.0), c13 = T(1.0 / 3.0);
-          r = cmk<C>(c23 * t.x + c13 * w.x, c23 * t.y + c13 * w.y);
-        }
-      }
-      out[c * u_comp + off] = r;
+      const C t = use_u ? cmk<C>(uc.x + dd * d.x, uc.y + dd * d.y) : d;
+      const C w = wc_[c];
+      out[c * u_comp + off] = cmk<C>(ct * t.x + cw * w.x, ct * t.y + cw * w.y);
     }
   };
 #pragma unroll
