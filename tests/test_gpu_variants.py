@@ -113,3 +113,21 @@ def test_dudt_every_row_padding(mask, prec, dim, N, monkeypatch):
     d_out = torch.empty_like(d_u)
     eq.dudt(d_out, d_u)
     assert rel_l2(to_host(d_out), ref) <= TOL[prec]
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("dim,N,M", [(3, 34, 384), (2, 34, 768)])
+def test_dudt_heavy_padding(prec, dim, N, M):
+    """Heavy padding (M far above 3N/2): narrow epilogue tiles of a few mode
+    columns, a partial last tile (N = 34 gives odd tile counts), and zero rows
+    filling most of every padded line."""
+    og = ora.Grid(dim, N, M)
+    g = az.Grid(dim, N, M)
+    oeq = ora.IncompressibleEuler(og, ora.make_viscosity(VISC_CFGS["smooth"], og))
+    u_hat = random_field_hat(dim, N, seed=700 + 10 * dim + N)
+    ref = oeq.dudt(u_hat)
+    eq = az.IncompressibleEuler(g, az.make_viscosity(VISC_CFGS["smooth"], g), prec)
+    d_u = to_dev(u_hat, prec)
+    d_out = torch.empty_like(d_u)
+    eq.dudt(d_out, d_u, 0.0, 0.0, 0.2)
+    assert rel_l2(to_host(d_out), ref) <= TOL[prec]
