@@ -129,12 +129,14 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-def ncu_traffic(kernel_key):
-    """DRAM bytes per launch of a kernel from the committed ncu summary, or None."""
+def ncu_traffic(kernel_key, table=None):
+    """DRAM bytes per launch of a kernel from the committed ncu summary, or
+    None; with `table`, that sub-table's entry for the kernel instead."""
     path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     try:
         with open(path) as f:
-            return json.load(f).get(kernel_key)
+            d = json.load(f)
+        return d.get(table, {}).get(kernel_key) if table else d.get(kernel_key)
     except Exception:
         return None
 
@@ -268,6 +270,7 @@ def run_ours(args, rank, world, local):
     traffic = ncu_traffic(kernel_keys[dom])
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "kernel": pass_names[dom],
+                "shared_pipe_pct": ncu_traffic(kernel_keys[dom], "_shared_pipe_pct"),
                 "peak_source": peak_kind, "passes": passes,
                 "step_bytes_model_gb": sum(by) / K / 1e9,
                 "step_gbs_model": sum(by) / K / (ms_per_step * 1e-3) / 1e9}
