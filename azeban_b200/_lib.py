@@ -33,7 +33,7 @@ EXPORTS = [
     "az_leray", "az_profile_enable", "az_profile_read", "az_euler_dudt_noalloc",
     "az_tune_set", "az_tune_get", "az_euler_diagnostics",
     "az_sim_member_start", "az_sim_member_stop", "az_group_create", "az_group_destroy",
-    "az_group_steps", "az_group_set_end", "az_group_simulate_until",
+    "az_group_steps", "az_group_steps_active", "az_group_set_end", "az_group_simulate_until",
 ]
 
 
@@ -103,6 +103,7 @@ def _load():
         "az_group_create": (I, [ct.POINTER(P), I, ct.POINTER(P)]),
         "az_group_destroy": (I, [P]),
         "az_group_steps": (I, [P, I, P]),
+        "az_group_steps_active": (I, [P, I, ct.POINTER(I), P]),
         "az_group_set_end": (I, [P, D, P]),
         "az_group_simulate_until": (I, [P, D, P]),
     }

@@ -394,8 +394,17 @@ class Group:
             lib.az_group_destroy(h)
             self._h = None
 
-    def steps(self, n: int, stream=None):
-        check(lib.az_group_steps(self._h, int(n), _stream_ptr(stream)))
+    def steps(self, n: int, stream=None, active=None):
+        """n SSP-RK3 steps.  active: optional per-simulation counts; only
+        members [0, active[i]) of simulation i are launched (none for 0), so
+        every started member must lie inside its prefix."""
+        if active is None:
+            check(lib.az_group_steps(self._h, int(n), _stream_ptr(stream)))
+            return
+        if len(active) != len(self.sims):
+            raise ValueError("active needs one count per simulation")
+        arr = (ct.c_int * len(self.sims))(*[int(a) for a in active])
+        check(lib.az_group_steps_active(self._h, int(n), arr, _stream_ptr(stream)))
 
     def set_end(self, t: float, stream=None):
         check(lib.az_group_set_end(self._h, float(t), _stream_ptr(stream)))

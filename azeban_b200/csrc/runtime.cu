@@ -340,6 +340,9 @@ size_t az_euler_workspace_size(az_euler e) { return e ? e->work_bytes : 0; }
 
 namespace azb {
 
+// Members the step kernels launch over: a prefix [0, n) of the batch.
+static inline int launch_members(az_euler e) { return e->nlaunch > 0 ? e->nlaunch : e->batch; }
+
 // The contiguous-axis product pass over every member.  Bits of the tuned
 // variant: 0 the radix plan, 1 the bulk-copy kernel (k_zpass) instead of
 // k_rows_product.
@@ -352,7 +355,7 @@ static cudaError_t product_pass(az_euler e, int dim, const RowArgs& r, cudaStrea
     z.tw = r.tw;
     z.nlines = r.nlines;
     z.nh = r.nh;
-    z.nmem = e->batch;
+    z.nmem = launch_members(e);
     z.in_line = int(r.in_line);
     z.out_line = int(r.out_line);
     z.in_mem = r.in_mem;
@@ -362,7 +365,8 @@ static cudaError_t product_pass(az_euler e, int dim, const RowArgs& r, cudaStrea
     return ks->zpass(e->v_rows & 1, dim, z, st);
   }
   const int nlp = dim == 3 ? ks->tiles[e->v_rows & 1].nlp3 : ks->tiles[e->v_rows & 1].nlp2;
-  return ks->rows_product(e->v_rows & 1, dim, r, unsigned(cdiv(r.nlines, 2 * nlp)), unsigned(e->batch), st);
+  return ks->rows_product(e->v_rows & 1, dim, r, unsigned(cdiv(r.nlines, 2 * nlp)), unsigned(launch_members(e)),
+                          st);
 }
 
 // One right-hand side of every member: out <- stage(mode, u, u0, RHS(u)).
@@ -371,7 +375,7 @@ static az_status rhs(az_euler e, const void* u, const void* u0, void* out, int m
                      double C, cudaStream_t st) {
   const KernelSet* ks = e->ks;
   const long long N = e->N, M = e->M, Nh = e->Nh;
-  const unsigned B = unsigned(e->batch);
+  const unsigned B = unsigned(launch_members(e));
   const int nc = ks->tiles[e->v_cols & 1].nc;
   cudaError_t ce;
   if (e->dim == 3) {
@@ -723,6 +727,9 @@ struct az_sim_s {
   // the same graph replays every step.
   cudaGraphExec_t exec = nullptr;
   bool graph_failed = false;
+  // The same step over a prefix [0, n) of the members, per n (groups'
+  // active-prefix steps).
+  std::map<int, cudaGraphExec_t> exec_prefix;
 };
 
 az_status az_sim_create(az_rk3 ts, double C, const void* u_init, void* stream, az_sim* out) {
@@ -760,6 +767,7 @@ az_status az_sim_create(az_rk3 ts, double C, const void* u_init, void* stream, a
 az_status az_sim_destroy(az_sim s) {
   if (!s) return AZ_OK;
   if (s->exec) cudaGraphExecDestroy(s->exec);
+  for (auto& kv : s->exec_prefix) cudaGraphExecDestroy(kv.second);
   cudaFree(s->u);
   cudaFreeHost(s->host);
   delete s;
@@ -793,12 +801,13 @@ static double visc_cap(az_euler e, double C) {
 
 static az_status sim_step(az_sim s, cudaStream_t st) {
   az_euler e = s->ts->eq;
-  const unsigned g = unsigned(cdiv(e->batch, 128));
-  k_ctrl_begin_sim<<<g, 128, 0, st>>>(e->ctrl, e->batch, visc_cap(e, s->C));
+  const int nb = launch_members(e);
+  const unsigned g = unsigned(cdiv(nb, 128));
+  k_ctrl_begin_sim<<<g, 128, 0, st>>>(e->ctrl, nb, visc_cap(e, s->C));
   AZB_CUDA(cudaGetLastError());
   az_status r = rk3_stages(s->ts, s->u, s->C, st);
   if (r != AZ_OK) return r;
-  k_ctrl_end<<<g, 128, 0, st>>>(e->ctrl, e->batch);
+  k_ctrl_end<<<g, 128, 0, st>>>(e->ctrl, nb);
   AZB_CUDA(cudaGetLastError());
   return AZ_OK;
 }
@@ -843,6 +852,53 @@ static az_status sim_run_steps(az_sim s, int n, cudaStream_t st) {
     if (r != AZ_OK) return r;
   }
   return AZ_OK;
+}
+
+// Captures one step over members [0, n) into a graph (once per n); nullptr
+// when graphs are unusable (per-pass profiling, failed capture), and the
+// caller then launches eagerly.
+static cudaGraphExec_t sim_graph_prefix(az_sim s, int n) {
+  if (g_prof || s->graph_failed) return nullptr;
+  auto it = s->exec_prefix.find(n);
+  if (it != s->exec_prefix.end()) return it->second;
+  az_euler e = s->ts->eq;
+  cudaStream_t cap = nullptr;
+  if (cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t ex = nullptr;
+  e->nlaunch = n;
+  bool ok = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+  if (ok) {
+    const az_status st = sim_step(s, cap);
+    const cudaError_t ce = cudaStreamEndCapture(cap, &g);
+    ok = st == AZ_OK && ce == cudaSuccess && g != nullptr;
+  }
+  e->nlaunch = 0;
+  if (ok) ok = cudaGraphInstantiate(&ex, g, 0) == cudaSuccess;
+  if (g) cudaGraphDestroy(g);
+  cudaStreamDestroy(cap);
+  if (!ok) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  s->exec_prefix[n] = ex;
+  return ex;
+}
+
+static az_status sim_steps_prefix(az_sim s, int n, int nsteps, cudaStream_t st) {
+  if (cudaGraphExec_t ex = sim_graph_prefix(s, n)) {
+    for (int i = 0; i < nsteps; ++i) AZB_CUDA(cudaGraphLaunch(ex, st));
+    return AZ_OK;
+  }
+  az_euler e = s->ts->eq;
+  e->nlaunch = n;
+  az_status r = AZ_OK;
+  for (int i = 0; i < nsteps && r == AZ_OK; ++i) r = sim_step(s, st);
+  e->nlaunch = 0;
+  return r;
 }
 }  // namespace azb
 
@@ -935,7 +991,22 @@ az_status az_sim_member_stop(az_sim s, int member, void* stream) {
 struct az_group_s {
   std::vector<az_sim> sims;
   cudaGraphExec_t exec = nullptr;
+  // Branch streams and events of the active-prefix steps.
+  std::vector<cudaStream_t> br;
+  std::vector<cudaEvent_t> join;
+  cudaEvent_t fork = nullptr;
 };
+
+static void group_free_branches(az_group g) {
+  for (cudaStream_t b : g->br)
+    if (b) cudaStreamDestroy(b);
+  for (cudaEvent_t j : g->join)
+    if (j) cudaEventDestroy(j);
+  if (g->fork) cudaEventDestroy(g->fork);
+  g->br.clear();
+  g->join.clear();
+  g->fork = nullptr;
+}
 
 az_status az_group_create(az_sim* sims, int n, az_group* out) {
   if (!sims || n < 1 || !out) return fail(AZ_ERR_INVALID, "az_group_create: bad argument");
@@ -979,8 +1050,18 @@ az_status az_group_create(az_sim* sims, int n, az_group* out) {
   }
   if (fork) cudaEventDestroy(fork);
   if (root) cudaStreamDestroy(root);
+  if (ok) {
+    g->br.assign(n, nullptr);
+    g->join.assign(n, nullptr);
+    ok = cudaEventCreateWithFlags(&g->fork, cudaEventDisableTiming) == cudaSuccess;
+    for (int i = 0; ok && i < n; ++i)
+      ok = cudaStreamCreateWithFlags(&g->br[i], cudaStreamNonBlocking) == cudaSuccess &&
+           cudaEventCreateWithFlags(&g->join[i], cudaEventDisableTiming) == cudaSuccess;
+  }
   if (!ok) {
     const cudaError_t last = cudaGetLastError();
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    group_free_branches(g);
     delete g;
     if (step_status != AZ_OK) return step_status;
     return fail(AZ_ERR_CUDA, std::string("az_group_create: graph capture failed: ") + cudaGetErrorString(last));
@@ -992,6 +1073,7 @@ az_status az_group_create(az_sim* sims, int n, az_group* out) {
 az_status az_group_destroy(az_group g) {
   if (!g) return AZ_OK;
   if (g->exec) cudaGraphExecDestroy(g->exec);
+  group_free_branches(g);
   delete g;
   return AZ_OK;
 }
@@ -1000,6 +1082,31 @@ az_status az_group_steps(az_group g, int nsteps, void* stream) {
   if (!g || nsteps < 0) return fail(AZ_ERR_INVALID, "az_group_steps: bad argument");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   for (int i = 0; i < nsteps; ++i) AZB_CUDA(cudaGraphLaunch(g->exec, st));
+  return AZ_OK;
+}
+
+az_status az_group_steps_active(az_group g, int nsteps, const int* nactive, void* stream) {
+  if (!g || nsteps < 0 || !nactive) return fail(AZ_ERR_INVALID, "az_group_steps_active: bad argument");
+  const int n = int(g->sims.size());
+  for (int i = 0; i < n; ++i)
+    if (nactive[i] < 0 || nactive[i] > g->sims[i]->ts->eq->batch)
+      return fail(AZ_ERR_INVALID, "az_group_steps_active: active count out of range");
+  if (nsteps == 0) return AZ_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  AZB_CUDA(cudaEventRecord(g->fork, st));
+  for (int i = 0; i < n; ++i) {
+    if (nactive[i] == 0) continue;
+    // Prefixes are rounded up to powers of two, so few graphs are captured.
+    const int batch = g->sims[i]->ts->eq->batch;
+    int nb = 1;
+    while (nb < nactive[i]) nb <<= 1;
+    if (nb > batch) nb = batch;
+    AZB_CUDA(cudaStreamWaitEvent(g->br[i], g->fork, 0));
+    const az_status r = sim_steps_prefix(g->sims[i], nb, nsteps, g->br[i]);
+    if (r != AZ_OK) return r;
+    AZB_CUDA(cudaEventRecord(g->join[i], g->br[i]));
+    AZB_CUDA(cudaStreamWaitEvent(st, g->join[i], 0));
+  }
   return AZ_OK;
 }
 

@@ -10,6 +10,10 @@
 
 struct az_euler_s {
   int dim, prec, batch;
+  // Members the step kernels launch over (0: all of batch).  Set only while a
+  // step is captured for a group's active prefix; members past it are not
+  // touched.
+  int nlaunch = 0;
   long long N, M, Nh;
   azb::Visc visc;
   double eps_visc;  // Equation::visc()

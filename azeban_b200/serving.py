@@ -4,8 +4,11 @@ Requests (one solve each: a 2-D double shear layer or a 3-D fractional
 Brownian field, an N, an end time and a seed) arrive over time.  Each size
 class (dim, N) owns a pool of slots: one batched IncompressibleEuler /
 SSP_RK3 / Simulation whose members are the slots.  All pools are advanced
-together, one SSP-RK3 step per tick, by one captured graph (``Group``); a
-slot whose clock reached its end is skipped on the device.  Between ticks the
+together, one SSP-RK3 step per tick (``Group``): each pool's step launches
+over its lowest slots only, up to the highest slot in use (slots are handed
+out lowest first), so a tick costs what the admitted solves cost, not what
+every slot of every pool would; a slot whose clock reached its end is skipped
+on the device.  Between ticks the
 host admits waiting requests into free slots (their state is generated on the
 device straight into the slot) and retires finished ones, so requests that
 arrive while others run join at the next step and their work overlaps.
@@ -133,7 +136,9 @@ class ServingLoop:
             sim = Simulation(g, C, ts, zeros)
             for b in range(cap):
                 sim.member_stop(b)
-            self.pools[cls] = {"eq": eq, "ts": ts, "sim": sim, "free": list(range(cap))[::-1],
+            # free slots as a min-heap: admissions take the lowest slot, which
+            # keeps the pool's active prefix short
+            self.pools[cls] = {"eq": eq, "ts": ts, "sim": sim, "free": list(range(cap)),
                                "active": {}, "cap": cap}
             sims.append(sim)
         torch.cuda.synchronize()
@@ -165,7 +170,7 @@ class ServingLoop:
                 if pool is None:
                     raise ValueError(f"no pool for class {(r.dim, r.N)}")
                 if pool["free"]:
-                    slot = pool["free"].pop()
+                    slot = heapq.heappop(pool["free"])
                     u0 = initial_state(r, self.precision)
                     pool["sim"].member_start(slot, u0, r.t_end)
                     pool["active"][slot] = r
@@ -179,7 +184,8 @@ class ServingLoop:
                 if i < len(pending):
                     time.sleep(max(0.0, min(0.01, pending[i].arrival - (time.perf_counter() - t0))))
                 continue
-            self.group.steps(1)
+            self.group.steps(1, active=[max(p["active"]) + 1 if p["active"] else 0
+                                        for p in self.pools.values()])
             steps_done += 1
             member_steps += sum(len(p["active"]) for p in self.pools.values())
             # retire finished members
@@ -196,7 +202,7 @@ class ServingLoop:
                     if keep_results:
                         results[r.rid] = pool["sim"].u()[slot].clone()
                     pool["sim"].member_stop(slot)
-                    pool["free"].append(slot)
+                    heapq.heappush(pool["free"], slot)
         wall = time.perf_counter() - t0
         lat = np.array([r["finish"] - r["arrival"] for r in records.values() if "finish" in r])
         done_steps = sum(r.get("steps", 0) for r in records.values())

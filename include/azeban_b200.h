@@ -163,6 +163,13 @@ az_status az_group_create(az_sim* sims, int n, az_group* out);
 az_status az_group_destroy(az_group g);
 /* nsteps graph launches; a member whose clock reached its end is skipped. */
 az_status az_group_steps(az_group g, int nsteps, void* stream);
+/* nsteps steps of members [0, nactive[i]) of simulation i only (none when
+ * nactive[i] is 0), each simulation on its own branch; members past the
+ * prefix are not touched, so every started member must lie inside it.  The
+ * kernels launch over the prefix rounded up to a power of two (a step graph
+ * per rounded prefix is captured on first use): a continuous-batching loop
+ * then pays for the slots in use, not for every slot of every pool. */
+az_status az_group_steps_active(az_group g, int nsteps, const int* nactive, void* stream);
 /* Sets every member's end to t (no step). */
 az_status az_group_set_end(az_group g, double t, void* stream);
 /* simulate_until for every member of every simulation of the group. */

@@ -107,3 +107,33 @@ def test_serving_matches_oracle_fp64():
     got = res[0].cpu().numpy()
     # the slot's last step is clamped to land on t_end, as simulate_until's is
     assert rel_l2(got, osim.u_) <= 1e-9
+
+
+def test_group_active_prefix_steps_match_full_steps():
+    """Steps over each simulation's active prefix give the members inside it
+    exactly what full steps give, leave the members past it untouched, and
+    skip a simulation whose prefix is empty."""
+    dim, N, B = 2, 32, 5
+    f = [random_field_hat(dim, N, seed=40 + b) for b in range(B)]
+    g3 = [random_field_hat(3, 16, seed=60 + b) for b in range(2)]
+    eq, ts, sim = _sim(dim, N, "f64", f)
+    eq2, ts2, ref = _sim(dim, N, "f64", f)
+    eq3, ts3, other = _sim(3, 16, "f64", g3)
+    grp = az.Group([sim, other])
+    full = az.Group([ref])
+    for gg in (grp, full):
+        gg.set_end(1.0)
+    for s in (sim, ref):
+        s.member_stop(3)
+        s.member_stop(4)
+    before_other = to_host(other.u())
+    grp.steps(6, active=[3, 0])
+    full.steps(6)
+    got, want = to_host(sim.u()), to_host(ref.u())
+    np.testing.assert_array_equal(got[:3], want[:3])
+    np.testing.assert_array_equal(got[3:], np.stack(f[3:]))
+    np.testing.assert_array_equal(to_host(other.u()), before_other)
+    assert sim.state()[1] == ref.state()[1] == [6, 6, 6, 0, 0]
+    assert other.state()[1] == [0, 0]
+    with pytest.raises(az.AzebanError):
+        grp.steps(1, active=[B + 1, 0])
