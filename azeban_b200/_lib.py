@@ -30,6 +30,7 @@ EXPORTS = [
     "az_sim_create", "az_sim_destroy", "az_sim_simulate_until", "az_sim_steps", "az_sim_u",
     "az_sim_state",
     "az_fft_create", "az_fft_destroy", "az_fft_forward", "az_fft_backward", "az_fft_work_area_size",
+    "az_fft_set_work_area",
     "az_leray", "az_profile_enable", "az_profile_read", "az_euler_dudt_noalloc",
     "az_tune_set", "az_tune_get", "az_euler_diagnostics",
     "az_sim_member_start", "az_sim_member_stop", "az_group_create", "az_group_destroy",
@@ -91,6 +92,7 @@ def _load():
         "az_fft_forward": (I, [P, P]),
         "az_fft_backward": (I, [P, P]),
         "az_fft_work_area_size": (SZ, [P]),
+        "az_fft_set_work_area": (I, [P, P]),
         "az_leray": (I, [I, LL, I, P, I, P]),
         "az_profile_enable": (I, [I]),
         "az_profile_read": (I, [ct.POINTER(D), ct.POINTER(D), ct.POINTER(LL), I]),

@@ -483,6 +483,17 @@ class FFT:
     def get_work_area_size(self):
         return lib.az_fft_work_area_size(self._h)
 
+    def set_work_area(self, work: torch.Tensor):
+        """FFT::set_work_area (fft.hpp:84): a device tensor of at least
+        get_work_area_size() bytes, used instead of an allocation of the
+        FFT's own; kept alive by the FFT."""
+        if not isinstance(work, torch.Tensor) or not work.is_cuda or not work.is_contiguous():
+            raise ValueError("work must be a contiguous CUDA tensor")
+        if work.numel() * work.element_size() < self.get_work_area_size():
+            raise ValueError("work area too small")
+        check(lib.az_fft_set_work_area(self._h, work.data_ptr()))
+        self._work = work
+
     def forward(self, stream=None):
         check(lib.az_fft_forward(self._h, _stream_ptr(stream)))
 

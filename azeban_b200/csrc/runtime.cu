@@ -1238,6 +1238,7 @@ struct az_fft_s {
   void* u;
   void* work = nullptr;
   size_t work_bytes = 0;
+  bool owns_work = false;  // allocated here (on the first backward transform)
   size_t csize;
 };
 
@@ -1279,22 +1280,27 @@ az_status az_fft_create(const az_fft_desc* d, void* u_hat, void* u, az_fft* out)
   f->nh = d->shape[d->dim - 1] / 2 + 1;
   long long celems = f->n_vars * f->nh;
   for (int a = 0; a < d->dim - 1; ++a) celems *= d->shape[a];
-  if (f->nt > 1) {
-    f->work_bytes = size_t(celems) * f->csize;
-    if (cudaMalloc(&f->work, f->work_bytes) != cudaSuccess) {
-      cudaGetLastError();
-      delete f;
-      return fail(AZ_ERR_NOMEM, "az_fft_create: work area");
-    }
-  }
+  // Only backward transforms over more than one axis use a work area; it is
+  // allocated on the first of them unless az_fft_set_work_area gave one, so
+  // a forward-only FFT never allocates (nor frees: cudaFree waits for the
+  // whole device).
+  if (f->nt > 1) f->work_bytes = size_t(celems) * f->csize;
   *out = f;
   return AZ_OK;
 }
 
 az_status az_fft_destroy(az_fft f) {
   if (!f) return AZ_OK;
-  cudaFree(f->work);
+  if (f->owns_work) cudaFree(f->work);
   delete f;
+  return AZ_OK;
+}
+
+az_status az_fft_set_work_area(az_fft f, void* work) {
+  if (!f || !work) return fail(AZ_ERR_INVALID, "az_fft_set_work_area: null argument");
+  if (f->owns_work) cudaFree(f->work);
+  f->work = work;
+  f->owns_work = false;
   return AZ_OK;
 }
 
@@ -1371,6 +1377,14 @@ az_status az_fft_backward(az_fft f, void* stream) {
   if (!(f->direction & AZ_FFT_BACKWARD)) return fail(AZ_ERR_INVALID, "FFT was not planned for backward transforms");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const int last = f->dim - 1;
+  if (f->work_bytes > 0 && f->work == nullptr) {
+    if (cudaMalloc(&f->work, f->work_bytes) != cudaSuccess) {
+      cudaGetLastError();
+      f->work = nullptr;
+      return fail(AZ_ERR_NOMEM, "az_fft_backward: work area");
+    }
+    f->owns_work = true;
+  }
   const void* src = f->u_hat;
   for (int ax = f->dim - f->nt; ax < last; ++ax) {
     az_status s = fft_axis(f, ax, src, f->work, COLK_PLAIN_INV, st);

@@ -189,10 +189,14 @@ typedef struct {
   int direction;           /* AZ_FFT_FORWARD | AZ_FFT_BACKWARD */
 } az_fft_desc;
 
-/* make_fft + FFT::initialize(u_hat, u): binds the arrays and allocates the
- * work area. */
+/* make_fft + FFT::initialize(u_hat, u): binds the arrays.  The work area
+ * (backward transforms over more than one axis only) is allocated on the
+ * first backward transform unless az_fft_set_work_area gave one. */
 az_status az_fft_create(const az_fft_desc* desc, void* u_hat, void* u, az_fft* out);
 az_status az_fft_destroy(az_fft fft);
+/* FFT::set_work_area (fft.hpp:84): a caller-owned device buffer of
+ * az_fft_work_area_size bytes, used instead of an allocation of its own. */
+az_status az_fft_set_work_area(az_fft fft, void* work);
 /* FFT::forward: u_hat <- unnormalised r2c(u) (fft.hpp:95). */
 az_status az_fft_forward(az_fft fft, void* stream);
 /* FFT::backward: u <- unnormalised c2r(u_hat) (fft.hpp:96); u_hat is kept. */

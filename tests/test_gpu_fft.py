@@ -97,3 +97,31 @@ def test_fft_unsupported_length_raises():
     u_hat = torch.zeros((1, 6), dtype=torch.complex128, device="cuda")
     with pytest.raises(az.AzebanError):
         az.make_fft(u_hat, u)
+
+
+def test_fft_caller_work_area():
+    """FFT::set_work_area (fft.hpp:84): a backward transform through a
+    caller-owned work area equals one through the FFT's own (allocated on
+    the first backward transform); a forward-only FFT reports its size but
+    allocates nothing."""
+    rng = np.random.default_rng(5)
+    u_np = rng.standard_normal((3, 24, 32, 16))
+    u_hat = torch.zeros((3, 24, 32, 9), dtype=torch.complex128, device="cuda")
+    u = torch.from_numpy(u_np).cuda()
+    own = az.make_fft(u_hat, u)
+    own.forward()
+    size = own.get_work_area_size()
+    assert size == 3 * 24 * 32 * 9 * 16
+    ref_hat = u_hat.clone()
+    out_own = torch.empty_like(u)
+    f_own = az.make_fft(ref_hat.clone(), out_own)
+    f_own.backward()
+    out_set = torch.empty_like(u)
+    f_set = az.make_fft(ref_hat.clone(), out_set)
+    work = torch.empty(size, dtype=torch.uint8, device="cuda")
+    f_set.set_work_area(work)
+    f_set.backward()
+    np.testing.assert_array_equal(out_set.cpu().numpy(), out_own.cpu().numpy())
+    assert rel_l2(out_set.cpu().numpy() / (24 * 32 * 16), u_np) <= 1e-13
+    with pytest.raises(ValueError):
+        f_set.set_work_area(torch.empty(size - 1, dtype=torch.uint8, device="cuda"))
