@@ -1126,9 +1126,15 @@ az_status az_group_simulate_until(az_group g, double t, void* stream) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   az_status r = az_group_set_end(g, t, stream);
   if (r != AZ_OK) return r;
+  // Each chunk steps only the members up to each simulation's last unfinished
+  // one (none once a simulation is done), so a simulation that finished
+  // early costs nothing while the others run on.
+  const int n = int(g->sims.size());
+  std::vector<int> active(n);
+  for (int i = 0; i < n; ++i) active[i] = g->sims[i]->ts->eq->batch;
   int chunk = 1;
   for (;;) {
-    r = az_group_steps(g, chunk, stream);
+    r = az_group_steps_active(g, chunk, active.data(), stream);
     if (r != AZ_OK) return r;
     double min_left = INFINITY;
     bool any = false;
@@ -1137,12 +1143,15 @@ az_status az_group_simulate_until(az_group g, double t, void* stream) {
       AZB_CUDA(cudaMemcpyAsync(s->host, e->ctrl, sizeof(Ctrl) * e->batch, cudaMemcpyDeviceToHost, st));
     }
     AZB_CUDA(cudaStreamSynchronize(st));
-    for (az_sim s : g->sims) {
+    for (int i = 0; i < n; ++i) {
+      az_sim s = g->sims[i];
       az_euler e = s->ts->eq;
+      active[i] = 0;
       for (int b = 0; b < e->batch; ++b) {
         if (s->host[b].err) return ctrl_error(s->host[b].err);
         if (s->host[b].time < t) {
           any = true;
+          active[i] = b + 1;
           const double dt = s->host[b].dt;
           const double left = dt > 0 ? (t - s->host[b].time) / dt : 1.0;
           if (left < min_left) min_left = left;

@@ -172,7 +172,9 @@ az_status az_group_steps(az_group g, int nsteps, void* stream);
 az_status az_group_steps_active(az_group g, int nsteps, const int* nactive, void* stream);
 /* Sets every member's end to t (no step). */
 az_status az_group_set_end(az_group g, double t, void* stream);
-/* simulate_until for every member of every simulation of the group. */
+/* simulate_until for every member of every simulation of the group; each
+ * chunk of steps launches only the simulations with unfinished members, over
+ * their members up to the last unfinished one. */
 az_status az_group_simulate_until(az_group g, double t, void* stream);
 
 /* ---- FFT<Dim> (include/azeban/operations/fft.hpp:37-121,
