@@ -60,7 +60,9 @@ template <typename T, int L, int DIM, int V> struct ZTile {
   static constexpr int CB = int(sizeof(cvec<T>));
   static constexpr int NB = DIM * (DIM + 1) / 2;
   static constexpr int TPL = Plan<L, V>::TPL;
-  static constexpr int BUDGET = kclamp(kpow2floor(81920 / (L * NB * CB)), 1, 16);
+  // About 80 KB of work area; 40 KB from L = 768 on, where the twiddle table
+  // and the longer lines would otherwise leave room for one CTA per SM.
+  static constexpr int BUDGET = kclamp(kpow2floor((L >= 768 ? 40960 : 81920) / (L * NB * CB)), 1, 16);
   static constexpr int G = (TPL % 32 == 0) ? 32 : (TPL % 16 == 0) ? 16 : (TPL % 8 == 0) ? 8
                          : (TPL % 4 == 0) ? 4 : (TPL % 2 == 0) ? 2 : 1;  // gcd(TPL, 32)
   static constexpr int MIN = DIM == 3 ? (G >= 16 ? 1 : 16 / G) : 32 / G;
