@@ -136,7 +136,6 @@ class ServingLoop:
         self.precision = precision
         self.C = C
         self.pools = {}
-        sims = []
         for cls, cap in capacities.items():
             if cap < 1:
                 continue
@@ -156,9 +155,7 @@ class ServingLoop:
             self.pools[cls] = {"eq": eq, "ts": ts, "sim": sim, "free": list(range(cap)),
                                "active": {}, "cap": cap, "stream": stream, "group": Group([sim]),
                                "step_bytes": member_step_bytes(dim, N, precision)}
-            sims.append(sim)
         torch.cuda.synchronize()
-        self.group = Group(sims)
         self._warm()
 
     def _warm(self):
