@@ -417,6 +417,15 @@ __global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NLP * Plan<L, V>::TPL)
   }
 }
 
+// Layout of one member's state: element (component c, retained row i, mode
+// p) at c * comp + i * row + p * ps.  Planar, the reference's [d][N]..[Nh]:
+// comp = N^{d-1} Nh, row = N^{d-2} Nh, ps = 1.  Component innermost,
+// [N]..[Nh][d] (the stepper's stage buffers): comp = 1, row = d N^{d-2} Nh,
+// ps = d, so a tile's few modes are d times more contiguous bytes per row.
+struct StateLayout {
+  int comp, row, ps;
+};
+
 struct EpiArgs {
   const void* B;  // [M][modes][NB], component innermost
   const void* u;
@@ -427,7 +436,8 @@ struct EpiArgs {
   int ntile;
   int N, nh;
   long long B_row, B_mem;
-  long long u_row, u_comp, u_mem;
+  StateLayout lu, lu0, lout;  // layouts of u, u0 and out
+  long long u_mem;
   int mode;
   Visc visc;
   const Ctrl* ctrl;
@@ -535,7 +545,7 @@ __global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NCM * Plan<L, V>::TPL,
   const C* u = reinterpret_cast<const C*>(a.u) + member * a.u_mem;
   const C* u0 = reinterpret_cast<const C*>(a.u0) + member * a.u_mem;
   C* out = reinterpret_cast<C*>(a.out) + member * a.u_mem;
-  const int u_row = int(a.u_row), u_comp = int(a.u_comp);  // a member's state < 2^31 elements
+  const StateLayout lu = a.lu, lu0 = a.lu0, lout = a.lout;  // offsets < 2^31, checked by the launcher
   const T inv_k0sq = T(1.0 / (a.visc.k0 * a.visc.k0));
   // The stage combination as uniform coefficients instead of per-element
   // branches: t = u + dt d (d itself for MODE_DUDT), r = ct t + cw u0.
@@ -571,16 +581,16 @@ __global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NCM * Plan<L, V>::TPL,
   for (int it = 0; it < MAXIT; ++it) {
     const int i = i0 + it * ISTEP;
     if (i < N) {
-      const int off = i * u_row + p;
+      const int ou = i * lu.row + p * lu.ps, ow = i * lu0.row + p * lu0.ps;
 #pragma unroll
       for (int c = 0; c < DIM; ++c) {
-        uv[it][c] = u[c * u_comp + off];
-        wv[it][c] = need_u0 ? u0[c * u_comp + off] : cmk<C>(T(0), T(0));
+        uv[it][c] = u[c * lu.comp + ou];
+        wv[it][c] = need_u0 ? u0[c * lu0.comp + ow] : cmk<C>(T(0), T(0));
       }
     }
   }
   auto process = [&](int i, const C (&uc_)[DIM], const C (&wc_)[DIM]) {
-    const int off = i * u_row + p;
+    const int oo = i * lout.row + p * lout.ps;
     const int i_ = i >= N / 2 + 1 ? i - N : i;
     const T k1 = twopi * T(i_);
     C Bv[NB];
@@ -632,7 +642,7 @@ __global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NCM * Plan<L, V>::TPL,
       const C d = zero ? cmk<C>(T(0), T(0)) : cmk<C>(-Lh[c].x + nu * uc.x, -Lh[c].y + nu * uc.y);
       const C t = use_u ? cmk<C>(uc.x + dd * d.x, uc.y + dd * d.y) : d;
       const C w = wc_[c];
-      out[c * u_comp + off] = cmk<C>(ct * t.x + cw * w.x, ct * t.y + cw * w.y);
+      out[c * lout.comp + oo] = cmk<C>(ct * t.x + cw * w.x, ct * t.y + cw * w.y);
     }
   };
 #pragma unroll
@@ -641,12 +651,12 @@ __global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NCM * Plan<L, V>::TPL,
     if (i < N) process(i, uv[it], wv[it]);
   }
   for (int i = i0 + MAXIT * ISTEP; i < N; i += ISTEP) {
-    const int off = i * u_row + p;
+    const int ou = i * lu.row + p * lu.ps, ow = i * lu0.row + p * lu0.ps;
     C uc[DIM], wc[DIM];
 #pragma unroll
     for (int c = 0; c < DIM; ++c) {
-      uc[c] = u[c * u_comp + off];
-      wc[c] = need_u0 ? u0[c * u_comp + off] : cmk<C>(T(0), T(0));
+      uc[c] = u[c * lu.comp + ou];
+      wc[c] = need_u0 ? u0[c * lu0.comp + ow] : cmk<C>(T(0), T(0));
     }
     process(i, uc, wc);
   }

@@ -201,7 +201,10 @@ template <typename T, int L, int V> struct LaunchV {
   static cudaError_t epi(int dim, const EpiArgs& a, dim3 g, cudaStream_t st) {
     // 32-bit offsets: rows of B and one member's state.
     const long long lim = 0x7fffffffLL;
-    if ((long long)L * a.B_row >= lim || (long long)dim * a.u_comp >= lim) return cudaErrorInvalidValue;
+    if ((long long)L * a.B_row >= lim) return cudaErrorInvalidValue;
+    for (const StateLayout& l : {a.lu, a.lu0, a.lout})
+      if ((long long)(dim - 1) * l.comp + (long long)(a.N - 1) * l.row + (a.ninner - 1) * l.ps >= lim)
+        return cudaErrorInvalidValue;
     if (dim == 2) return epi_kernel<2, TS::NCM2>(a, g, st);
     if (dim == 3) return epi_kernel<3, TS::NCM3>(a, g, st);
     return cudaErrorInvalidValue;

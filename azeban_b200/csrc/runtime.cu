@@ -369,10 +369,24 @@ static cudaError_t product_pass(az_euler e, int dim, const RowArgs& r, cudaStrea
                           st);
 }
 
+// A member's state layout: planar (the reference's [d][N]..[Nh], every array
+// a caller passes) or component innermost ([N]..[Nh][d], the stepper's own
+// stage buffers: the pass-1 reads and the epilogue's state accesses of a
+// tile of a few modes are then d times wider per row).
+static StateLayout state_layout(az_euler e, bool inner) {
+  const long long N = e->N, Nh = e->Nh;
+  const int d = e->dim;
+  const long long plane = d == 3 ? N * Nh : Nh;  // modes of one retained row
+  if (inner) return StateLayout{1, int(d * plane), d};
+  return StateLayout{int(d == 3 ? N * N * Nh : N * Nh), int(plane), 1};
+}
+
 // One right-hand side of every member: out <- stage(mode, u, u0, RHS(u)).
 // first_stage: compute dt = min(C/(N u_max), max_dt) after the product pass.
-static az_status rhs(az_euler e, const void* u, const void* u0, void* out, int mode, bool first_stage,
-                     double C, cudaStream_t st) {
+// u_inner / u0_inner / out_inner: the array is in the component-innermost
+// layout (else planar).
+static az_status rhs(az_euler e, const void* u, bool u_inner, const void* u0, bool u0_inner, void* out,
+                     bool out_inner, int mode, bool first_stage, double C, cudaStream_t st) {
   const KernelSet* ks = e->ks;
   const long long N = e->N, M = e->M, Nh = e->Nh;
   const unsigned B = unsigned(launch_members(e));
@@ -388,15 +402,17 @@ static az_status rhs(az_euler e, const void* u, const void* u0, void* out, int m
     a1.ninner = N * e->ra1;
     a1.ntile = int(cdiv(a1.ninner, nc));
     a1.n_short = int(N);
-    a1.in_row = N * Nh;
+    a1.in_row = u_inner ? 3 * N * Nh : N * Nh;
     a1.out_row = N * e->ra1;
     if (e->ra1 != 3 * Nh) {
       a1.grp = int(e->ra1);
       a1.grp_valid = int(3 * Nh);
-      a1.in_grp = Nh;
+      a1.in_grp = u_inner ? 3 * Nh : Nh;
     }
-    a1.in_comp = N * N * Nh;
-    a1.in_ci = 3;
+    // component innermost: entry q = 3 z + component is already the input's
+    // order, so the columns read straight runs
+    a1.in_comp = u_inner ? 0 : N * N * Nh;
+    a1.in_ci = u_inner ? 1 : 3;
     a1.in_mem = e->state_mem;
     a1.out_mem = e->buf_mem[0];
     a1.ctrl = e->ctrl;
@@ -454,10 +470,10 @@ static az_status rhs(az_euler e, const void* u, const void* u0, void* out, int m
     a1.ninner = 2 * Nh;
     a1.ntile = int(cdiv(a1.ninner, nc));
     a1.n_short = int(N);
-    a1.in_row = Nh;
+    a1.in_row = u_inner ? 2 * Nh : Nh;
     a1.out_row = e->ra1;
-    a1.in_comp = N * Nh;
-    a1.in_ci = 2;
+    a1.in_comp = u_inner ? 0 : N * Nh;
+    a1.in_ci = u_inner ? 1 : 2;
     a1.in_mem = e->state_mem;
     a1.out_mem = e->buf_mem[0];
     a1.ctrl = e->ctrl;
@@ -539,8 +555,9 @@ static az_status rhs(az_euler e, const void* u, const void* u0, void* out, int m
   ep.B_row = b_row;
   ep.B_mem = b_mem;
   ep.b_grp = (e->dim == 3 && e->rb2 != 6 * Nh) ? e->rb2 : 0;
-  ep.u_row = e->dim == 3 ? N * Nh : Nh;
-  ep.u_comp = e->dim == 3 ? N * N * Nh : N * Nh;
+  ep.lu = state_layout(e, u_inner);
+  ep.lu0 = u0 ? state_layout(e, u0_inner) : ep.lu;
+  ep.lout = state_layout(e, out_inner);
   ep.u_mem = e->state_mem;
   ep.mode = mode;
   ep.visc = e->visc;
@@ -568,14 +585,14 @@ az_status az_euler_dudt(az_euler e, void* dudt_hat, const void* u_hat, double t,
   // A plain right-hand side: clear any skip flag left by a finished simulation.
   k_ctrl_begin_host<<<unsigned(cdiv(e->batch, 128)), 128, 0, st>>>(e->ctrl, e->batch, 0.0);
   AZB_CUDA(cudaGetLastError());
-  return rhs(e, u_hat, nullptr, dudt_hat, MODE_DUDT, false, C, st);
+  return rhs(e, u_hat, false, nullptr, false, dudt_hat, false, MODE_DUDT, false, C, st);
 }
 
 namespace azb {
 az_status euler_dudt_launch(az_euler e, void* dudt_hat, const void* u_hat, cudaStream_t st) {
   k_ctrl_begin_host<<<unsigned(cdiv(e->batch, 128)), 128, 0, st>>>(e->ctrl, e->batch, 0.0);
   AZB_CUDA(cudaGetLastError());
-  return rhs(e, u_hat, nullptr, dudt_hat, MODE_DUDT, false, 0.0, st);
+  return rhs(e, u_hat, false, nullptr, false, dudt_hat, false, MODE_DUDT, false, 0.0, st);
 }
 az_status set_error(az_status st, const char* msg) { return fail(st, msg); }
 const KernelSet* find_kernel_set(int precision, int L) { return kernel_set(precision, L); }
@@ -686,11 +703,13 @@ namespace azb {
 static az_status rk3_stages(az_rk3 r, void* u, double C, cudaStream_t st) {
   az_euler e = r->eq;
   az_status s;
-  s = rhs(e, u, nullptr, r->u1, MODE_RK1, true, C, st);
+  // u (the caller's) is planar; the stage buffers u1 and u2 are component
+  // innermost.
+  s = rhs(e, u, false, nullptr, false, r->u1, true, MODE_RK1, true, C, st);
   if (s != AZ_OK) return s;
-  s = rhs(e, r->u1, u, r->u2, MODE_RK2, false, C, st);
+  s = rhs(e, r->u1, true, u, false, r->u2, true, MODE_RK2, false, C, st);
   if (s != AZ_OK) return s;
-  return rhs(e, r->u2, u, u, MODE_RK3, false, C, st);
+  return rhs(e, r->u2, true, u, false, u, false, MODE_RK3, false, C, st);
 }
 }  // namespace azb
 
