@@ -465,14 +465,26 @@ def run_tg3d_accuracy(args):
                                        u32.to(torch.complex128).contiguous())}
         times = [(i + 1) / (10 * 2 * math.pi) for i in range(10)] + [1.0]
         rows = []
+        busy_ms = {"fp32": 0.0, "fp64": 0.0}
         for t in times:
-            for s_ in sims.values():
+            for name, s_ in sims.items():
+                e0, e1 = _ev(), _ev()
+                e0.record()
                 s_.simulate_until(t)
+                e1.record()
+                torch.cuda.synchronize()
+                if name in busy_ms:
+                    busy_ms[name] += e0.elapsed_time(e1)
             ref = sims["fp64"].u()
             nrm = torch.linalg.vector_norm(ref)
             rows.append({"t": t, "l2_fp32_vs_fp64": float(torch.linalg.vector_norm(sims["fp32"].u().to(torch.complex128) - ref) / nrm),
                          "floor": float(torch.linalg.vector_norm(sims["floor"].u() - ref) / nrm)})
-        out.append({"N": N, "outputs": rows})
+        # one member each, stepped to t = 1 (azeban units) through simulate_until
+        rate = {}
+        for name, ms in busy_ms.items():
+            steps = sims[name].state()[1][0]
+            rate[name] = {"steps": steps, "ms_per_step": ms / steps, "member_steps_per_s": steps / (ms / 1e3)}
+        out.append({"N": N, "outputs": rows, "throughput_one_member": rate})
         del sims
     print(json.dumps({"workload": "TG-3D accuracy FP32 bulk vs FP64", "results": out}), flush=True)
 
