@@ -378,8 +378,11 @@ class Simulation:
 
 
 class Group:
-    """Several simulations (any dimension, size, precision) advanced together,
-    one captured graph per SSP-RK3 step with one branch per simulation."""
+    """Several simulations (any dimension, size, precision) advanced together:
+    steps() replays one captured graph per SSP-RK3 step with a branch per
+    simulation; steps(active=...) and simulate_until() launch, per
+    simulation, a step graph over its active member prefix only (none for a
+    finished simulation), each on its own stream."""
 
     def __init__(self, sims):
         self.sims = list(sims)
