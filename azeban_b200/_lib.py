@@ -13,13 +13,14 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libazeban_b200.so")
 
 AZ_OK = 0
+AZ_ERR_INVALID, AZ_ERR_UNSUPPORTED, AZ_ERR_CUDA, AZ_ERR_NOMEM, AZ_ERR_NONFINITE, AZ_ERR_TIMEOUT = 1, 2, 3, 4, 5, 6
 AZ_PREC_F64, AZ_PREC_F32 = 0, 1
 AZ_VISC_NONE, AZ_VISC_SMOOTH_CUTOFF, AZ_VISC_STEP, AZ_VISC_QUADRATIC = 0, 1, 2, 3
 AZ_FFT_FORWARD, AZ_FFT_BACKWARD = 1, 2
 AZ_NOALLOC_SCRATCH_BYTES = 64 * 1024 * 1024
 
 STATUS_NAMES = {0: "AZ_OK", 1: "AZ_ERR_INVALID", 2: "AZ_ERR_UNSUPPORTED", 3: "AZ_ERR_CUDA",
-                4: "AZ_ERR_NOMEM", 5: "AZ_ERR_NONFINITE"}
+                4: "AZ_ERR_NOMEM", 5: "AZ_ERR_NONFINITE", 6: "AZ_ERR_TIMEOUT"}
 
 # Every entry point include/azeban_b200.h declares.
 EXPORTS = [
@@ -35,6 +36,7 @@ EXPORTS = [
     "az_tune_set", "az_tune_get", "az_euler_diagnostics",
     "az_sim_member_start", "az_sim_member_stop", "az_group_create", "az_group_destroy",
     "az_group_steps", "az_group_steps_active", "az_group_set_end", "az_group_simulate_until",
+    "az_debug_set_wait_limit", "az_debug_get_wait_limit", "az_euler_noalloc_status",
 ]
 
 
@@ -108,6 +110,9 @@ def _load():
         "az_group_steps_active": (I, [P, I, ct.POINTER(I), P]),
         "az_group_set_end": (I, [P, D, P]),
         "az_group_simulate_until": (I, [P, D, P]),
+        "az_debug_set_wait_limit": (I, [I]),
+        "az_debug_get_wait_limit": (I, []),
+        "az_euler_noalloc_status": (I, [P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

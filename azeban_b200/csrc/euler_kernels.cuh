@@ -286,19 +286,21 @@ __global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NLP * Plan<L, V>::TPL)
   load_twiddles<C, L>(tw, reinterpret_cast<const C*>(a.tw));
   __syncthreads();
 
-  // 1. Inverse transforms.  Column col = (pair p, slot q) holds signal 2q +
-  //    i * signal 2q+1, signal s = component s % DIM of line s / DIM of the
-  //    pair; its first stage reads global memory directly.
+  // 1. Inverse transforms.  Column col = (pair p, component q) holds
+  //    component q of line 2p + i * component q of line 2p+1 (the same
+  //    component of two neighbouring lines, so the two real signals sharing
+  //    a transform have like magnitudes and neither inherits the other's
+  //    rounding); its first stage reads global memory directly.
   {
     const bool active = tid < NINV * TPL;
     const int col = active ? tid % NINV : 0;
     const int tl = active ? tid / NINV : 0;
     const int p = col / DIM;
     const int q = col % DIM;
-    const long long l0 = line0 + 2 * p + (2 * q) / DIM;
-    const long long l1 = line0 + 2 * p + (2 * q + 1) / DIM;
-    const C* src0 = (active && l0 < a.nlines) ? in + l0 * a.in_line + (2 * q) % DIM : nullptr;
-    const C* src1 = (active && l1 < a.nlines) ? in + l1 * a.in_line + (2 * q + 1) % DIM : nullptr;
+    const long long l0 = line0 + 2 * p;
+    const long long l1 = l0 + 1;
+    const C* src0 = (active && l0 < a.nlines) ? in + l0 * a.in_line + q : nullptr;
+    const C* src1 = (active && l1 < a.nlines) ? in + l1 * a.in_line + q : nullptr;
     const int nh = a.nh;
     fft_columns<C, +1, L, SROW, true, P>(
         sm, tw, col, tl,
@@ -322,11 +324,12 @@ __global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NLP * Plan<L, V>::TPL)
     if (idx < NLP * L) {
       const int m = idx % L;
       const int p = idx / L;
+      // sv[it][0, DIM): components of line a, [DIM, 2 DIM): of line b
 #pragma unroll
       for (int q = 0; q < DIM; ++q) {
         const C z = sm[m * SROW + p * DIM + q];
-        sv[it][2 * q] = z.x;
-        sv[it][2 * q + 1] = z.y;
+        sv[it][q] = z.x;
+        sv[it][DIM + q] = z.y;
       }
 #pragma unroll
       for (int s = 0; s < 2 * DIM; ++s) {
@@ -347,7 +350,7 @@ __global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NLP * Plan<L, V>::TPL)
       T pa[NB], pb[NB];
       if constexpr (DIM == 2) {
         const T a1 = norm * sv[it][0], a2 = norm * sv[it][1];
-        const T b1 = norm * sv[it][2], b2 = norm * sv[it][3];
+        const T b1 = norm * sv[it][2], b2 = norm * sv[it][3];  // line b
         pa[0] = a1 * a1; pa[1] = a1 * a2; pa[2] = a2 * a2;
         pb[0] = b1 * b1; pb[1] = b1 * b2; pb[2] = b2 * b2;
       } else {

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include "euler_kernels.cuh"
+#include "zfused.cuh"
 #include "zpass.cuh"
 
 namespace azb {
@@ -32,6 +33,8 @@ struct KernelSet {
   cudaError_t (*rows_product)(int v, int dim, const RowArgs&, unsigned gx, unsigned gy, cudaStream_t);
   // Bulk-copy form of the product pass (plan variant v & 1).
   cudaError_t (*zpass)(int v, int dim, const ZArgs&, cudaStream_t);
+  // Fused product pass (bit 0: forward plan, bit 1: inverse plan).
+  cudaError_t (*zfused)(int v, int dim, const ZArgs&, cudaStream_t);
   cudaError_t (*epilogue)(int v, int dim, const EpiArgs&, unsigned gx, unsigned gy, cudaStream_t);
   cudaError_t (*c2r)(int v, const RealRowArgs&, unsigned gx, cudaStream_t);
   cudaError_t (*r2c)(int v, const RealRowArgs&, unsigned gx, cudaStream_t);
@@ -52,6 +55,21 @@ template <typename T, int L, int V> struct Tiles {
   static constexpr int NCM3 = kclamp(kpow2floor(81920 / (L * 6 * CB)), 1, 16);
   static constexpr int NCM2 = kclamp(kpow2floor(81920 / (L * 3 * CB)), 1, 16);
   static constexpr int NLPR = kclamp(kpow2floor(49152 / (L * CB)), 1, 64);
+};
+
+// Line pairs per chunk of k_zfused: a work area (gap rows included) of about
+// 80 KB, raised until the CTA's thread count is a whole number of warps.
+template <typename T, int L, int DIM, int VF> struct ZFTile {
+  static constexpr int CB = int(sizeof(cvec<T>));
+  static constexpr int NB = DIM * (DIM + 1) / 2;
+  static constexpr int TPL = Plan<L, VF>::TPL;
+  static constexpr int ROWS = Rows16<1>::nrows(L);
+  static constexpr int BUDGET = kclamp(kpow2floor(81920 / (ROWS * NB * CB)), 1, 16);
+  static constexpr int G = (TPL % 32 == 0) ? 32 : (TPL % 16 == 0) ? 16 : (TPL % 8 == 0) ? 8
+                         : (TPL % 4 == 0) ? 4 : (TPL % 2 == 0) ? 2 : 1;  // gcd(TPL, 32)
+  static constexpr int MIN = DIM == 3 ? (G >= 16 ? 1 : 16 / G) : 32 / G;
+  static constexpr int NLP = BUDGET > MIN ? BUDGET : MIN;
+  static_assert((NB * NLP * TPL) % 32 == 0, "k_zfused needs whole warps");
 };
 
 // Line pairs per chunk of k_zpass: about 80 KB of work area, raised until the
@@ -187,6 +205,44 @@ template <typename T, int L, int V> struct LaunchV {
     return cudaErrorInvalidValue;
   }
 
+  // k_zfused with forward plan V (this struct's) and inverse plan VI.
+  template <int DIM, int VI>
+  static cudaError_t zfused(const ZArgs& a0, cudaStream_t st) {
+    constexpr int NLP = ZFTile<T, L, DIM, V>::NLP;
+    using Z = ZFShape<T, L, NLP, DIM, V, VI>;
+    auto k = k_zfused<T, L, NLP, DIM, V, VI>;
+    if (a0.in_line < a0.nh * DIM || a0.out_line < a0.nh * Z::NB) return cudaErrorInvalidValue;
+    // Each pair's bulk copy needs 16-byte aligned source, destination and size.
+    const long long pair_bytes = 2LL * a0.in_line * Z::CB;
+    if ((reinterpret_cast<uintptr_t>(a0.in) & 15) != 0 || pair_bytes % 16 != 0 ||
+        (a0.in_mem * Z::CB) % 16 != 0 || (a0.nlines & 1) != 0)
+      return cudaErrorInvalidValue;
+    ZArgs a = a0;
+    a.pstride = zfused_pair_stride(a.in_line, Z::CB, NLP, DIM, Z::CS, Z::NINV);
+    const long long smem = Z::smem_bytes(a.pstride);
+    if (smem > 227 * 1024) return cudaErrorInvalidValue;
+    static long long granted = 48 * 1024;
+    if (smem > granted) {
+      const cudaError_t ce = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+      if (ce != cudaSuccess) {
+        cudaGetLastError();
+        return ce;
+      }
+      granted = smem;
+    }
+    const long long chunks = (a.nlines + 2 * NLP - 1) / (2 * NLP);
+    if (chunks == 0 || a.nmem == 0) return cudaSuccess;
+    if (chunks > 0x7fffffffLL || a.nmem > 65535) return cudaErrorInvalidValue;
+    k<<<dim3(unsigned(chunks), unsigned(a.nmem)), Z::NT, size_t(smem), st>>>(a);
+    return cudaGetLastError();
+  }
+
+  static cudaError_t zfused(int vi, int dim, const ZArgs& a, cudaStream_t st) {
+    if (dim == 2) return vi ? zfused<2, 1>(a, st) : zfused<2, 0>(a, st);
+    if (dim == 3) return vi ? zfused<3, 1>(a, st) : zfused<3, 0>(a, st);
+    return cudaErrorInvalidValue;
+  }
+
   template <int DIM, int NCM>
   static cudaError_t epi_kernel(const EpiArgs& a, dim3 g, cudaStream_t st) {
     constexpr int NB = DIM * (DIM + 1) / 2;
@@ -252,6 +308,11 @@ template <typename T, int L> struct Launch {
   static cudaError_t zpass(int v, int dim, const ZArgs& a, cudaStream_t st) {
     return (v & 1) ? LaunchV<T, L, 1>::zpass(dim, a, st) : LaunchV<T, L, 0>::zpass(dim, a, st);
   }
+  // v bit 0: forward plan, bit 1: inverse plan
+  static cudaError_t zfused(int v, int dim, const ZArgs& a, cudaStream_t st) {
+    const int vi = (v >> 1) & 1;
+    return (v & 1) ? LaunchV<T, L, 1>::zfused(vi, dim, a, st) : LaunchV<T, L, 0>::zfused(vi, dim, a, st);
+  }
   static cudaError_t epilogue(int v, int dim, const EpiArgs& a, unsigned gx, unsigned gy,
                               cudaStream_t st) {
     const dim3 g(gx, gy, 1);
@@ -270,6 +331,7 @@ template <typename T, int L> struct Launch {
                                  &cols,
                                  &rows_product,
                                  &zpass,
+                                 &zfused,
                                  &epilogue,
                                  &c2r,
                                  &r2c};

@@ -10,16 +10,22 @@
 //
 // The array is a static __device__ variable: every GPU that loads the library
 // holds it until the process exits.  Host code cannot use its name as a device
-// address, so the first call on each device (with that device current) looks
-// the address up with cudaGetSymbolAddress and keeps it; make that first call
-// before any stream capture.  All calls share the one array and it keeps the
-// last call's contents, so each call rewrites everything it reads (control
-// block, twiddle table) before use.  Calls whose work overlaps on the GPU
-// (other streams, other host threads) race on the array.
+// address, so every call looks the address up on the current device with
+// cudaGetSymbolAddress (a lookup the runtime answers from its module table
+// after the first call, which may load the module: make the first call on a
+// device before any stream capture).  Looking it up each time keeps the
+// address right after a cudaDeviceReset, which loads the module anew.  All
+// calls share the one array and it keeps the last call's contents, so each
+// call rewrites everything it reads (control block, twiddle table) before
+// use.  Calls whose work overlaps on the GPU (other streams, other host
+// threads) race on the array.  The kernels report device-side failures (a
+// non-finite velocity, a bounded wait that ran out) in the control block at
+// the start of the array; az_euler_noalloc_status reads it, allocating
+// nothing either.
 #include <cuda_runtime.h>
 
 #include <cmath>
-#include <mutex>
+#include <cstddef>
 #include <string>
 
 #include "runtime_internal.h"
@@ -28,24 +34,13 @@ namespace azb {
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[AZ_NOALLOC_SCRATCH_BYTES];
 
-static std::mutex g_noalloc_mutex;
-static void* g_noalloc_ptr[64] = {};
-
 // Device address of g_noalloc_scratch on the current device.
 static az_status noalloc_scratch(void** out) {
-  int dev = 0;
-  cudaError_t ce = cudaGetDevice(&dev);
-  if (ce != cudaSuccess) return set_error(AZ_ERR_CUDA, cudaGetErrorString(ce));
-  if (dev < 0 || dev >= 64) return set_error(AZ_ERR_UNSUPPORTED, "az_euler_dudt_noalloc: device index >= 64");
-  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-  if (g_noalloc_ptr[dev] == nullptr) {
-    void* p = nullptr;
-    ce = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (ce != cudaSuccess)
-      return set_error(AZ_ERR_CUDA, (std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(ce)).c_str());
-    g_noalloc_ptr[dev] = p;
-  }
-  *out = g_noalloc_ptr[dev];
+  void* p = nullptr;
+  const cudaError_t ce = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (ce != cudaSuccess)
+    return set_error(AZ_ERR_CUDA, (std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(ce)).c_str());
+  *out = p;
   return AZ_OK;
 }
 
@@ -141,4 +136,19 @@ az_status az_euler_dudt_noalloc(int dim, long long N_phys, long long N_phys_pad,
   ce = cudaGetLastError();
   if (ce != cudaSuccess) return set_error(AZ_ERR_CUDA, cudaGetErrorString(ce));
   return euler_dudt_launch(&e, dudt_hat, u_hat, s);
+}
+
+az_status az_euler_noalloc_status(void* stream) {
+  void* base = nullptr;
+  az_status st = noalloc_scratch(&base);
+  if (st != AZ_OK) return st;
+  // The control block sits at the start of the array; its error word is the
+  // only part read.  The copy goes to a local (pageable) int: no allocation.
+  int err = 0;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cudaError_t ce = cudaMemcpyAsync(&err, static_cast<const char*>(base) + offsetof(Ctrl, err), sizeof(int),
+                                   cudaMemcpyDeviceToHost, s);
+  if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+  if (ce != cudaSuccess) return set_error(AZ_ERR_CUDA, cudaGetErrorString(ce));
+  return ctrl_status(err);
 }

@@ -60,7 +60,7 @@ int tuned_variant(int precision, int L, int kind) {
   if (const char* env = std::getenv("AZ_PLAN_VARIANT")) {
     int v[3] = {0, 0, 0};
     if (std::sscanf(env, "%d,%d,%d", &v[0], &v[1], &v[2]) == 3 && kind >= 0 && kind < 6)
-      return kind % 3 == 2 ? (v[2] & 1) : (v[kind % 3] & 3);
+      return kind % 3 == 2 ? (v[2] & 1) : (v[kind % 3] & (kind % 3 == 1 ? 7 : 3));
   }
   return precision == 1 ? 1 : 0;
 }
@@ -83,9 +83,14 @@ static az_status cuda_fail(cudaError_t e, const char* what) {
 // reduction, bit 1 a bounded wait on a kernel's own bulk copy that ran out
 // (the kernel then returned early and its output is incomplete).
 static az_status ctrl_error(int err) {
-  if (err & 2) return fail(AZ_ERR_CUDA, "a bulk-copy wait inside a transform pass ran out; the pass is incomplete");
+  if (err & 2)
+    return fail(AZ_ERR_TIMEOUT, "a bounded bulk-copy wait inside a transform pass ran out; the pass is incomplete");
   return fail(AZ_ERR_NONFINITE, "non-finite value in the CFL reduction");
 }
+
+// Polls of the product pass's bounded wait for its bulk copy (kWaitPolls
+// unless az_debug_set_wait_limit changed it).
+static int g_wait_polls = kWaitPolls;
 
 #define AZB_CUDA(call)                                   \
   do {                                                   \
@@ -227,7 +232,10 @@ void euler_layout(az_euler_s* e) {
     e->buf_mem[1] = M * M * e->ra2;                             // A2 [M][M][ra2]
     e->buf_mem[2] = M * M * e->rb1;                             // B1 [M][M][rb1]
     e->state_mem = 3 * N * N * Nh;
-    e->norm = 1.0 / (std::pow(std::sqrt((double)N), 3) * std::pow(std::sqrt((double)M), 3));
+    // 1 / (N^{3/2} M^{3/2}) with the integer powers by repeated
+    // multiplication, as computeB forms it (incompressible_euler.hpp:171-173)
+    const double sn = std::sqrt((double)N), sm = std::sqrt((double)M);
+    e->norm = 1.0 / ((sn * (sn * sn)) * (sm * (sm * sm)));
     e->Md = (double)(M * M * M);
   } else {
     e->ra1 = row(2 * Nh, 0);
@@ -238,7 +246,8 @@ void euler_layout(az_euler_s* e) {
     e->buf_mem[1] = M * e->rb1;  // B1 [M][rb1]
     e->buf_mem[2] = 0;
     e->state_mem = 2 * N * Nh;
-    e->norm = 1.0 / (std::pow(std::sqrt((double)N), 2) * std::pow(std::sqrt((double)M), 2));
+    const double sn = std::sqrt((double)N), sm = std::sqrt((double)M);
+    e->norm = 1.0 / ((sn * sn) * (sm * sm));
     e->Md = (double)(M * M);
   }
 }
@@ -348,7 +357,7 @@ static inline int launch_members(az_euler e) { return e->nlaunch > 0 ? e->nlaunc
 // k_rows_product.
 static cudaError_t product_pass(az_euler e, int dim, const RowArgs& r, cudaStream_t st) {
   const KernelSet* ks = e->ks;
-  if (e->v_rows & 2) {
+  if (e->v_rows & 6) {
     ZArgs z{};
     z.in = r.in;
     z.out = r.out;
@@ -362,6 +371,8 @@ static cudaError_t product_pass(az_euler e, int dim, const RowArgs& r, cudaStrea
     z.out_mem = r.out_mem;
     z.norm = r.norm;
     z.ctrl = r.ctrl;
+    z.wait_polls = g_wait_polls;
+    if (e->v_rows & 4) return ks->zfused(e->v_rows & 3, dim, z, st);
     return ks->zpass(e->v_rows & 1, dim, z, st);
   }
   const int nlp = dim == 3 ? ks->tiles[e->v_rows & 1].nlp3 : ks->tiles[e->v_rows & 1].nlp2;
@@ -596,7 +607,16 @@ az_status euler_dudt_launch(az_euler e, void* dudt_hat, const void* u_hat, cudaS
 }
 az_status set_error(az_status st, const char* msg) { return fail(st, msg); }
 const KernelSet* find_kernel_set(int precision, int L) { return kernel_set(precision, L); }
+az_status ctrl_status(int err) { return err ? ctrl_error(err) : AZ_OK; }
 }  // namespace azb
+
+az_status az_debug_set_wait_limit(int polls) {
+  if (polls < 0) return fail(AZ_ERR_INVALID, "az_debug_set_wait_limit: polls must be >= 0");
+  g_wait_polls = polls;
+  return AZ_OK;
+}
+
+int az_debug_get_wait_limit(void) { return g_wait_polls; }
 
 az_status az_euler_dt(az_euler e, double C, void* stream, double* out) {
   if (!e || !out) return fail(AZ_ERR_INVALID, "az_euler_dt: null argument");
@@ -622,7 +642,7 @@ az_status az_euler_dt(az_euler e, double C, void* stream, double* out) {
 }
 
 az_status az_tune_set(int precision, int L, int kind, int variant) {
-  const int vmax = kind % 3 == 2 ? 1 : 3;
+  const int vmax = kind % 3 == 2 ? 1 : kind % 3 == 1 ? 7 : 3;
   if ((precision != 0 && precision != 1) || kind < 0 || kind > 5 || variant < 0 || variant > vmax)
     return fail(AZ_ERR_INVALID, "az_tune_set: bad argument");
   if (!kernel_set(precision, L)) return fail(AZ_ERR_UNSUPPORTED, "az_tune_set: no compiled length");

@@ -52,6 +52,9 @@ void euler_layout(az_euler_s* e);
 az_status euler_dudt_launch(az_euler e, void* dudt_hat, const void* u_hat, cudaStream_t st);
 // Sets the thread's last-error string and returns st.
 az_status set_error(az_status st, const char* msg);
+// AZ_OK for a zero Ctrl::err word, else the status (and message) it encodes:
+// bit 1 AZ_ERR_TIMEOUT, bit 0 AZ_ERR_NONFINITE.
+az_status ctrl_status(int err);
 // Compiled kernels of one (precision, transform length), or nullptr.
 const KernelSet* find_kernel_set(int precision, int L);
 // Plan variant (0 std, 1 wide) the tuning table holds for a pass kind

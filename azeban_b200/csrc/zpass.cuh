@@ -8,7 +8,8 @@
 // thread issues a global load.  The inverse transform's first stage reads the
 // half spectra there directly, the Hermitian extension folded into its loads.
 // The mbarrier wait is bounded; a wait that runs out sets bit 1 of the
-// member's error word and the CTA returns.
+// member's error word, waits (bounded) for the copy to land, and the CTA
+// returns.
 //
 // Reference: the inverse transform, max_norm and computeB of
 // IncompressibleEuler::dudt (include/azeban/equations/incompressible_euler.hpp
@@ -44,10 +45,13 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned 
       : "memory");
   return ok != 0u;
 }
-// Bounded wait on one phase of an mbarrier; false if it never completed.
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
-  constexpr int kLimit = 1 << 22;
-  for (int i = 0; i < kLimit; ++i)
+// Polls of a bounded mbarrier wait (the default of ZArgs::wait_polls, and the
+// limit of the wait for an in-flight copy after a wait ran out).
+constexpr int kWaitPolls = 1 << 22;
+// Bounded wait on one phase of an mbarrier: at most `limit` polls; false if
+// the phase did not complete.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity, int limit) {
+  for (int i = 0; i < limit; ++i)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
@@ -103,6 +107,8 @@ struct ZArgs {
   long long in_mem, out_mem;  // member strides (elements)
   double norm;       // 1 / (N^{d/2} M^{d/2})
   Ctrl* ctrl;
+  int wait_polls;    // limit of the wait for the chunk's bulk copy (kWaitPolls)
+  int pstride;       // k_zfused: shared-memory elements between input line pairs
 };
 
 // Shared-memory layout of one CTA (bytes), shared by the kernel and its
@@ -202,9 +208,17 @@ __global__ void __launch_bounds__(ZShape<T, L, NLP, DIM, V>::NT, ZShape<T, L, NL
   }
   load_twiddles<C, L>(tw, reinterpret_cast<const C*>(a.tw));
   __syncthreads();
-  const bool ok = mbar_wait_bounded(&bar[0], 0u);
+  const bool ok = mbar_wait_bounded(&bar[0], 0u, a.wait_polls);
   if (__syncthreads_or(!ok)) {
-    if (tid == 0) atomicOr(&ctrl->err, 2);
+    // The wait ran out: flag it (bit 1 of the member's error word), and let
+    // one thread wait, bounded, for the copy to land before the CTA exits,
+    // so no bulk copy is still writing into shared memory the SM may hand to
+    // the next CTA.  The CTA's shared memory stays allocated until its last
+    // thread exits.
+    if (tid == 0) {
+      atomicOr(&ctrl->err, 2);
+      mbar_wait_bounded(&bar[0], 0u, kWaitPolls);
+    }
     return;
   }
   using AB = AbsBits<T>;

@@ -32,12 +32,17 @@ VISC = {"type": "Smooth Cutoff", "eps": 0.05}
 
 # Kernel variants: bit 0 picks the radix plan (0 std, 1 wide); bit 1 picks
 # the two-tile column kernel (column passes) or the bulk-copy kernel
-# (contiguous-axis pass).  The epilogue has plan variants only.
-RUNS = (0, 1, 2, 3)
+# (contiguous-axis pass).  Runs 4-7 time the fused product pass (bit 2 of
+# the contiguous-axis variant; its bit 1 is then the inverse transform's
+# plan); the other passes repeat runs 0-3 there.  The epilogue has plan
+# variants only.
+RUNS = (0, 1, 2, 3, 4, 5, 6, 7)
 
 
 def _kind_variant(kind0: int, run: int) -> int:
-    return run if kind0 in (0, 1) else run & 1
+    if kind0 == 1:
+        return run
+    return run & 3 if kind0 == 0 else run & 1
 
 
 def _set_all(prec: int, L: int, run: int) -> None:

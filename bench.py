@@ -59,6 +59,11 @@ def parse():
                     help="tg3d256 is the headline; the others are the remaining workloads, one JSON line each")
     ap.add_argument("--duration", type=float, default=60.0, help="serving: seconds of Poisson arrivals")
     ap.add_argument("--rate", type=float, default=200.0, help="serving: arrivals per second")
+    ap.add_argument("--dry-run", action="store_true",
+                    help="launch and rank bookkeeping only (gloo, no GPU): each rank reports in, rank 0 "
+                         "prints how many ranks took part")
+    ap.add_argument("--cpu-budget", type=float, default=150.0,
+                    help="--impl reference: seconds of timed whole SSP-RK3 steps at most")
     return ap.parse_args()
 
 
@@ -141,40 +146,77 @@ def ncu_traffic(kernel_key, table=None):
         return None
 
 
+class CpuStepper:
+    """Whole SSP-RK3 steps of one member with the oracle (FP64, scipy.fft on
+    `cores` threads): the CPU restatement of the reference's path.  The
+    oracle evaluates a 3-D right-hand side whole (dudt) or slab by slab
+    (dudt_slabs, the same arithmetic in a cache-friendlier order); the first
+    right-hand side times both and the faster one is used, so the baseline is
+    not held back by the evaluation order."""
+
+    def __init__(self, n, cores):
+        from oracle import euler_oracle as ora
+        self.ora = ora
+        ora.set_workers(cores)
+        g = ora.Grid(3, n)
+        self.eq = ora.IncompressibleEuler(g, ora.make_viscosity(VISC_CFG, g))
+        self.ts = ora.SSP_RK3(self.eq)
+        self.u = ora.initialize(ora.taylor_green_workload(3, n))
+        t0 = time.perf_counter()
+        self.eq.dudt(self.u)
+        t1 = time.perf_counter()
+        self.eq.dudt_slabs(self.u)
+        t2 = time.perf_counter()
+        self.eq.slabs = (t2 - t1) < (t1 - t0)
+        self.form = "slab by slab" if self.eq.slabs else "whole arrays"
+        self.cap = self.ora.math.inf if self.eq.visc() == 0 else \
+            C_CFL * 2.0 / (self.eq.visc() * (self.ora.PI * n) ** 2)
+
+    def step(self):
+        """One timed SSP-RK3 step; returns its seconds."""
+        t0 = time.perf_counter()
+        self.ts.integrate(0.0, self.cap, C_CFL, self.u)
+        return time.perf_counter() - t0
+
+
 def cpu_sample(n, cores):
-    """One right-hand side of one member with the oracle (FP64, scipy.fft on
-    `cores` threads); returns (seconds, member-steps in the sample)."""
-    from oracle import euler_oracle as ora
-    ora.set_workers(cores)
-    g = ora.Grid(3, n)
-    eq = ora.IncompressibleEuler(g, ora.make_viscosity(VISC_CFG, g))
-    u = ora.initialize(ora.taylor_green_workload(3, n))
-    t0 = time.perf_counter()
-    eq.dudt(u)
-    return time.perf_counter() - t0, 1.0 / 3.0
+    """One whole SSP-RK3 step of one 3-D member with the oracle; returns
+    (seconds, member-steps in the sample, stepper)."""
+    st = CpuStepper(n, cores)
+    return st.step(), 1.0, st
 
 
 def run_reference(args, rank, world):
+    """The reference arm: the oracle (the reference itself cannot be built
+    here) on all host cores, whole SSP-RK3 steps of one 256^3 member.  The
+    steps reported are the steps actually timed: at most --steps, and no
+    more than fit in --cpu-budget seconds (at least one)."""
     if rank != 0:
         return
     cores = os.cpu_count() or 1
+    t_start = time.perf_counter()
+    st = CpuStepper(args.n, cores)
+    st.step()  # warm-up step (plans, page faults); one is enough on the CPU
     samples = []
-    for i in range(args.warmup + args.steps):
-        sec, ms = cpu_sample(args.n, cores)
-        if i >= args.warmup:
-            samples.append(sec / ms)
+    while len(samples) < max(1, args.steps):
+        samples.append(st.step())
+        if sum(samples) + statistics.mean(samples) > args.cpu_budget:
+            break
     per_member_step = statistics.mean(samples)
     value = 1.0 / per_member_step
     line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_member_step * 1e3,
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": len(samples), "warmup": 1, "steps_requested": args.steps, "warmup_requested": args.warmup,
+        "ms_per_step": per_member_step * 1e3, "timed_s": sum(samples),
+        "run_s": time.perf_counter() - t_start,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
         "config": {"workload": f"TG-3D {args.n}^3, M={3 * args.n // 2}, SmoothCutoff eps=0.05, SSP-RK3, C=0.2",
                    "members": 1, "l2": "inputs larger than L2"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"one right-hand side of one {args.n}^3 member per step (1/3 member-step), "
-                                   "numpy/scipy.fft restatement of the reference CPU path"},
+                         "sample": f"{len(samples)} whole SSP-RK3 steps (3 right-hand sides each) of one "
+                                   f"{args.n}^3 member, FP64 numpy/scipy.fft restatement of the reference CPU "
+                                   f"path ({st.form}), after one warm-up step"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -376,10 +418,10 @@ def run_ours(args, rank, world, local):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cores = os.cpu_count() or 1
-        sec, msteps = cpu_sample(N, cores)
+        sec, msteps, cst = cpu_sample(N, cores)
         cpu = {"value": msteps / sec, "unit": UNIT, "cores": cores, "kind": "port",
-               "sample": f"one right-hand side of one {N}^3 member (1/3 member-step), FP64 numpy/scipy.fft "
-                         f"restatement of the reference CPU path, {sec:.1f} s"}
+               "sample": f"one whole SSP-RK3 step of one {N}^3 member, FP64 numpy/scipy.fft restatement of "
+                         f"the reference CPU path ({cst.form}), {sec:.1f} s"}
 
     launches_per_step = 1 + 3 * 5 + 1 + 1
     if rank == 0:
@@ -394,6 +436,12 @@ def run_ours(args, rank, world, local):
             "p50_step_ms": p50, "p99_step_ms": p99,
             "fp64": fp64,
             "fp32_over_fp64": (value / world) / fp64["member_steps_per_s"] * world if fp64 else None,
+            # The same precision on both sides: the plain FP64 GPU form against
+            # the FP64 CPU restatement, one member each.
+            "like_for_like_fp64": ({"gpu_member_steps_per_s": fp64["member_steps_per_s"] / world,
+                                    "cpu_member_steps_per_s": cpu["value"],
+                                    "gpu_over_cpu": fp64["member_steps_per_s"] / world / cpu["value"]}
+                                   if fp64 and cpu else None),
             "accuracy": accuracy,
             "e2e": e2e,
             "roofline": roofline,
@@ -643,9 +691,46 @@ def run_serving(args):
           flush=True)
 
 
+def launch_ranks(args):
+    """--gpus N without a launcher: re-run this command under
+    torch.distributed.run with N ranks on this node (one per GPU, rendezvous
+    on 127.0.0.1) and return its exit code."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+           "--master-addr=127.0.0.1", f"--master-port={port}", os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
+def run_dry(args, rank, world):
+    """Rank bookkeeping without a GPU: gloo ranks report in; rank 0 prints the
+    number that took part and the max over ranks of a per-rank value."""
+    import datetime
+
+    import torch.distributed as dist
+
+    from azeban_b200 import replicas
+    if world > 1:
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+    seen = int(replicas.sum_over_ranks(1.0, device="cpu"))
+    slowest = replicas.max_over_ranks(float(rank + 1), device="cpu")
+    if rank == 0:
+        print(json.dumps({"dry_run": True, "n_gpus": world, "ranks_seen": seen, "max_over_ranks": slowest,
+                          "members": replicas.partition_by_cost([1.0] * (4 * world), world)}), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(launch_ranks(args))
     rank, world, local = dist_env()
+    if args.dry_run:
+        run_dry(args, rank, world)
+        return
     if args.impl == "reference":
         run_reference(args, rank, world)
         return

@@ -28,7 +28,8 @@ typedef enum {
   AZ_ERR_UNSUPPORTED = 2, /* a size with no compiled transform length */
   AZ_ERR_CUDA = 3,        /* a CUDA runtime call failed */
   AZ_ERR_NOMEM = 4,       /* device allocation failed */
-  AZ_ERR_NONFINITE = 5    /* the CFL reduction met Inf or NaN */
+  AZ_ERR_NONFINITE = 5,   /* the CFL reduction met Inf or NaN */
+  AZ_ERR_TIMEOUT = 6      /* a bounded wait inside a kernel ran out; that pass is incomplete */
 } az_status;
 
 typedef enum { AZ_PREC_F64 = 0, AZ_PREC_F32 = 1 } az_precision;
@@ -234,6 +235,19 @@ az_status az_profile_enable(int on);
  * counts since the last read; npass >= 5.  Waits for the recorded events. */
 az_status az_profile_read(double* ms, double* bytes, long long* launches, int npass);
 
+/* ---- failure detection (no reference counterpart: the reference has no
+ *      in-kernel waits and aborts on errors, src/azeban/logging.hpp:24-32) */
+
+/* Polls of the bounded wait with which the product pass waits for its bulk
+ * copy (default 2^22).  A wait that runs out flags the member's error word;
+ * the kernel then waits for the copy to land and returns, and the next call
+ * that reads the error word (az_euler_dt, az_rk3_integrate, simulate_until,
+ * az_euler_noalloc_status) returns AZ_ERR_TIMEOUT.  0 makes every such wait
+ * run out at once: the way the tests exercise that path without a fault.
+ * Applies to launches (and graph captures) made after the call. */
+az_status az_debug_set_wait_limit(int polls);
+int az_debug_get_wait_limit(void);
+
 /* ---- leray (src/azeban/operations/leray.cpp:28-116) --------------------- */
 
 /* In-place projection of u_hat [batch][dim][N]([N])[N/2+1] onto divergence-free
@@ -254,11 +268,21 @@ az_status az_leray(int dim, long long N, int precision, void* u_hat, int batch, 
  * one file-scope device array of AZ_NOALLOC_SCRATCH_BYTES, held by every GPU
  * that loads the library until the process exits.  That bounds the sizes: at
  * 3/2 padding, 3-D up to N = 64 and 2-D up to N = 1024, in either precision;
- * a larger size returns AZ_ERR_UNSUPPORTED.  The first call on a device looks
- * up the array's device address; make it before any stream capture.  Every
- * call shares the array, so calls that overlap on the GPU race. */
+ * a larger size returns AZ_ERR_UNSUPPORTED.  Each call looks up the array's
+ * device address on the current device; the first call on a device may load
+ * the library's device code to do so, so make it before any stream capture.  Every
+ * call shares the array, so calls that overlap on the GPU race.  The call
+ * does not wait for the GPU: device-side failures are read with
+ * az_euler_noalloc_status. */
 az_status az_euler_dudt_noalloc(int dim, long long N_phys, long long N_phys_pad, int precision,
                                 const az_visc* visc, void* dudt_hat, const void* u_hat, void* stream);
+
+/* Device-side status of the last az_euler_dudt_noalloc on the current device,
+ * read from the control block in the same fixed array (no allocation):
+ * AZ_OK, AZ_ERR_NONFINITE (the CFL reduction met Inf or NaN) or
+ * AZ_ERR_TIMEOUT (a bounded wait ran out; the output is incomplete).
+ * Synchronises the stream.  It has no counterpart in the reference. */
+az_status az_euler_noalloc_status(void* stream);
 
 #ifdef __cplusplus
 }

@@ -58,6 +58,32 @@ def _rfftn(x, axes):
     return np.fft.rfftn(x, axes=axes, norm="backward")
 
 
+# Single-axis and partial transforms of the slab-wise right-hand side, with
+# the same unnormalised conventions (inverse unscaled, forward unscaled).
+def _ifftn(x, axes):
+    if _sfft is not None:
+        return _sfft.ifftn(x, axes=axes, norm="forward", workers=_WORKERS)
+    return np.fft.ifftn(x, axes=axes, norm="forward")
+
+
+def _irfft(x, n, axis):
+    if _sfft is not None:
+        return _sfft.irfft(x, n=n, axis=axis, norm="forward", workers=_WORKERS)
+    return np.fft.irfft(x, n=n, axis=axis, norm="forward")
+
+
+def _rfft(x, axis):
+    if _sfft is not None:
+        return _sfft.rfft(x, axis=axis, norm="backward", workers=_WORKERS)
+    return np.fft.rfft(x, axis=axis, norm="backward")
+
+
+def _fft(x, axis):
+    if _sfft is not None:
+        return _sfft.fft(x, axis=axis, norm="backward", workers=_WORKERS)
+    return np.fft.fft(x, axis=axis, norm="backward")
+
+
 # --------------------------------------------------------------------------
 # Grid (include/azeban/grid.hpp:30-165, include/azeban/grid_factory.hpp:28-92)
 # --------------------------------------------------------------------------
@@ -329,10 +355,12 @@ class IncompressibleEuler:
     """Equation<Dim> for the spectral-viscosity incompressible Euler RHS
     with no forcing (include/azeban/forcing/no_forcing.hpp:28-44)."""
 
-    def __init__(self, grid: Grid, visc):
+    def __init__(self, grid: Grid, visc, slabs: bool = False):
         self.grid = grid
         self.visc_ = visc
         self.u_max_ = 0.0
+        # 3-D: evaluate dudt() with the bounded-memory dudt_slabs()
+        self.slabs = bool(slabs) and grid.dim == 3
         d = grid.dim
         N, M = grid.N_phys, grid.N_phys_pad
         kk = [2 * PI * signed_index(N).astype(np.float64)] * (d - 1) + [
@@ -367,13 +395,22 @@ class IncompressibleEuler:
         """Padded inverse transform, N^d-scaled (incompressible_euler.hpp:115)."""
         return fft_backward(self.pad(u_hat), self.grid.N_phys_pad)
 
+    def norm(self) -> float:
+        """1 / (N^{d/2} M^{d/2}) as computeB forms it: the integer powers of
+        the square roots by repeated multiplication (incompressible_euler.hpp:171-173)."""
+        d = self.grid.dim
+        sn, sm = math.sqrt(self.grid.N_phys), math.sqrt(self.grid.N_phys_pad)
+        pn, pm = sn, sm
+        for _ in range(d - 1):
+            pn, pm = sn * pn, sm * pm
+        return 1.0 / (pn * pm)
+
     def compute_B(self, u):
         """Scale by 1/(N^{d/2} M^{d/2}) then the symmetric product in the
         reference's component order (incompressible_euler.hpp:168-213,
         incompressible_euler_functions.hpp:26-45)."""
         d = self.grid.dim
-        N, M = self.grid.N_phys, self.grid.N_phys_pad
-        norm = 1.0 / (math.sqrt(N) ** d * math.sqrt(M) ** d)
+        norm = self.norm()
         v = [norm * u[c] for c in range(d)]
         if d == 2:
             return np.stack([v[0] * v[0], v[0] * v[1], v[1] * v[1]])
@@ -391,44 +428,179 @@ class IncompressibleEuler:
         d = self.grid.dim
         if d == 2:
             Bs = B_hat[np.ix_(range(3), self._ret[0], self._ret[1])]
-            B11, B12, B22 = Bs[0], Bs[1], Bs[2]
             k1, k2 = self._k
-            b1 = 1j * k1 * B11 + 1j * k2 * B12
-            b2 = 1j * k1 * B12 + 1j * k2 * B22
-            with np.errstate(divide="ignore", invalid="ignore"):
-                inv = 1.0 / self._absk2
-            k11, k12, k22 = k1 * k1 * inv, k1 * k2 * inv, k2 * k2 * inv
-            L = [(1.0 - k11) * b1 + (0.0 - k12) * b2,
-                 (0.0 - k12) * b1 + (1.0 - k22) * b2]
-        else:
-            Bs = B_hat[np.ix_(range(6), self._ret[0], self._ret[1], self._ret[2])]
-            B11, B21, B22, B31, B32, B33 = (Bs[c] for c in range(6))
-            k1, k2, k3 = self._k
-            b1 = 1j * k1 * B11 + 1j * k2 * B21 + 1j * k3 * B31
-            b2 = 1j * k1 * B21 + 1j * k2 * B22 + 1j * k3 * B32
-            b3 = 1j * k1 * B31 + 1j * k2 * B32 + 1j * k3 * B33
-            with np.errstate(divide="ignore", invalid="ignore"):
-                inv = 1.0 / self._absk2
-            k11, k12, k13 = k1 * k1 * inv, k1 * k2 * inv, k1 * k3 * inv
-            k22, k23, k33 = k2 * k2 * inv, k2 * k3 * inv, k3 * k3 * inv
-            L = [(1.0 - k11) * b1 + (0.0 - k12) * b2 + (0.0 - k13) * b3,
-                 (0.0 - k12) * b1 + (1.0 - k22) * b2 + (0.0 - k23) * b3,
-                 (0.0 - k13) * b1 + (0.0 - k23) * b2 + (1.0 - k33) * b3]
-        zero = self._absk2 == 0
+            return _dudt_modes_2d(Bs, u_hat, k1, k2, self._absk2, self._nu)
+        Bs = B_hat[np.ix_(range(6), self._ret[0], self._ret[1], self._ret[2])]
+        k1, k2, k3 = self._k
+        return _dudt_modes_3d(Bs, u_hat, k1, k2, k3, self._absk2, self._nu)
+
+    def dudt_modes(self, signed_idx, B_modes, u_modes):
+        """The per-mode right-hand side for a list of modes (see dudt_modes)."""
+        return dudt_modes(self.visc_, signed_idx, B_modes, u_modes)
+
+    def dudt_single(self, u_hat):
+        """The same right-hand side with the padded transforms and the
+        products in single precision (pocketfft float32 and float32
+        products; the per-mode projection and viscosity stay FP64).  Not the
+        reference: a measure of how far any FP32 evaluation of a given
+        field's right-hand side lands from FP64, which the FP32-bulk parity
+        tests use as the conditioning of that field (fields whose nonlinear
+        terms cancel strongly carry FP32 errors above 1e-5 whatever the
+        FFT).  Leaves u_max_ unchanged."""
+        if self.grid.dim == 3:
+            keep = self.u_max_
+            out = self.dudt_slabs(u_hat, single=True)
+            self.u_max_ = keep
+            return out
+        d = self.grid.dim
+        M = self.grid.N_phys_pad
+        up = self.pad(u_hat).astype(np.complex64)
+        u = _irfftn(up, s=(M,) * d, axes=tuple(range(1, d + 1)))
+        norm = np.float32(self.norm())
+        v = [norm * u[c] for c in range(d)]
+        B = np.stack([v[0] * v[0], v[0] * v[1], v[1] * v[1]])
+        B_hat = _rfftn(B, axes=tuple(range(1, d + 1)))
+        return self.compute_dudt(B_hat.astype(np.complex128), u_hat)
+
+    def dudt_slabs(self, u_hat, xchunk=16, zchunk=16, colchunk=1 << 16, single=False):
+        """The same right-hand side as dudt() for 3-D, with bounded memory.
+
+        The padded transforms are split by axis: inverse along x and y per
+        chunk of z wavenumbers, then per chunk of x planes the c2r along z,
+        max |u|, B = u (x) u and the r2c along z and forward transform along
+        y (kept at the retained rows), then the forward transform along x and
+        the per-mode L and viscosity per chunk of (y, z) columns.  The padded
+        physical field never exists whole: the largest array is the
+        y-transformed product spectrum [6][M][N][N/2+1].  Used for sizes whose
+        padded arrays do not fit in host memory at once (N = 512, M = 768).
+        The transform order is the one pocketfft's irfftn / rfftn use, so the
+        result equals dudt() up to rounding.  Sets u_max_."""
+        if self.grid.dim != 3:
+            raise ValueError("dudt_slabs is for 3-D solves")
+        N, M = self.grid.N_phys, self.grid.N_phys_pad
+        Nh, Mh = N // 2 + 1, M // 2 + 1
+        pmap = pad_index_map_full(N, M)
+        dsel, ssel = np.nonzero(pmap >= 0)[0], pmap[pmap >= 0]
+        ret = retained_index_map(N, M)
+        cdt = np.complex64 if single else np.complex128
+        norm = np.float32(self.norm()) if single else self.norm()
+        xs = [np.arange(a, min(a + xchunk, M)) for a in range(0, M, xchunk)]
+        # 1. inverse along x and y of the padded spectrum, per z-wavenumber chunk
+        T = [np.empty((3, len(xc), M, Nh), dtype=cdt) for xc in xs]
+        for k0 in range(0, Nh, zchunk):
+            ks = slice(k0, min(k0 + zchunk, Nh))
+            src = u_hat[:, :, :, ks].astype(cdt)
+            pad = np.zeros((3, M, M, src.shape[-1]), dtype=cdt)
+            pad[np.ix_(range(3), dsel, dsel, range(src.shape[-1]))] = src[np.ix_(range(3), ssel, ssel,
+                                                                                 range(src.shape[-1]))]
+            t = _ifftn(pad, axes=(1, 2))
+            for i, xc in enumerate(xs):
+                T[i][:, :, :, ks] = t[:, xc]
+            del pad, t
+        # 2. per x chunk: c2r along z, max |u|, products, r2c along z, forward y
+        W = np.empty((6, M, N, Nh), dtype=cdt)
+        umax = 0.0
+        for i, xc in enumerate(xs):
+            ext = np.zeros((3, len(xc), M, Mh), dtype=cdt)
+            ext[..., :Nh] = T[i]
+            T[i] = None
+            u = _irfft(ext, M, axis=3)
+            del ext
+            umax = max(umax, float(np.max(np.abs(u))))
+            v = [norm * u[c] for c in range(3)]
+            del u
+            B = np.stack([v[0] * v[0], v[1] * v[0], v[1] * v[1], v[2] * v[0], v[2] * v[1], v[2] * v[2]])
+            del v
+            Bz = _rfft(B, axis=3)[..., :Nh]
+            del B
+            W[:, xc] = _fft(Bz, axis=2)[:, :, ret, :]
+            del Bz
+        self.u_max_ = umax / float(M ** 3)
+        # 3. forward along x per column chunk, then the per-mode right-hand side
+        W = W.reshape(6, M, N * Nh)
         out = np.empty_like(u_hat)
-        for c in range(d):
-            out[c] = np.where(zero, 0.0, -L[c] + self._nu * u_hat[c])
+        out_f = out.reshape(3, N, N * Nh)
+        u_f = u_hat.reshape(3, N, N * Nh)
+        k1 = (2 * PI * signed_index(N).astype(np.float64))[:, None]
+        for c0 in range(0, N * Nh, colchunk):
+            cs = slice(c0, min(c0 + colchunk, N * Nh))
+            Bx = _fft(W[:, :, cs], axis=1)[:, ret, :].astype(np.complex128)
+            col = np.arange(cs.start, cs.stop)
+            k2 = (2 * PI * signed_index(N).astype(np.float64)[col // Nh])[None, :]
+            k3 = (2 * PI * (col % Nh).astype(np.float64))[None, :]
+            absk2 = k1 * k1 + k2 * k2 + k3 * k3
+            nu = self.visc_.eval(np.sqrt(absk2))
+            out_f[:, :, cs] = _dudt_modes_3d(Bx, u_f[:, :, cs], k1, k2, k3, absk2, nu)
         return out
 
     def dudt(self, u_hat, t=0.0, dt=0.0, C=0.0):
         """One right-hand side (incompressible_euler.hpp:103-120).  Returns a
         new array; sets u_max_ as the reference does."""
+        if self.slabs:
+            return self.dudt_slabs(u_hat)
         d = self.grid.dim
         u = self.physical(u_hat)
         self.u_max_ = max_norm(u) / float(self.grid.N_phys_pad ** d)
         B = self.compute_B(u)
         B_hat = fft_forward(B)
         return self.compute_dudt(B_hat, u_hat)
+
+
+def dudt_modes(visc, signed_idx, B_modes, u_modes):
+    """The per-mode right-hand side for a list of modes: signed indices
+    [dim, n] (the last one the compact index), B_hat at those modes
+    [d(d+1)/2, n], u_hat [dim, n] (incompressible_euler.hpp:230-347)."""
+    d = len(signed_idx)
+    ks = [2 * PI * np.asarray(signed_idx[c], dtype=np.float64) for c in range(d)]
+    absk2 = ks[0] * ks[0]
+    for k in ks[1:]:
+        absk2 = absk2 + k * k
+    nu = visc.eval(np.sqrt(absk2))
+    if d == 2:
+        return _dudt_modes_2d(B_modes, u_modes, ks[0], ks[1], absk2, nu)
+    return _dudt_modes_3d(B_modes, u_modes, ks[0], ks[1], ks[2], absk2, nu)
+
+
+def _dudt_modes_2d(Bs, u_hat, k1, k2, absk2, nu):
+    """Per retained mode in 2-D: b = i k.B_hat, L = (I - k k^T/|k|^2) b,
+    dudt = -L + nu u_hat, zero at |k| = 0 (incompressible_euler_functions.hpp:47-71,
+    incompressible_euler.hpp:230-281).  Bs: (B11, B12, B22) at the modes."""
+    B11, B12, B22 = Bs[0], Bs[1], Bs[2]
+    b1 = 1j * k1 * B11 + 1j * k2 * B12
+    b2 = 1j * k1 * B12 + 1j * k2 * B22
+    with np.errstate(divide="ignore", invalid="ignore"):
+        inv = 1.0 / absk2
+        k11, k12, k22 = k1 * k1 * inv, k1 * k2 * inv, k2 * k2 * inv
+        L = [(1.0 - k11) * b1 + (0.0 - k12) * b2,
+             (0.0 - k12) * b1 + (1.0 - k22) * b2]
+        zero = absk2 == 0
+        out = np.empty(u_hat.shape, dtype=np.complex128)
+        for c in range(2):
+            out[c] = np.where(zero, 0.0, -L[c] + nu * u_hat[c])
+    return out
+
+
+def _dudt_modes_3d(Bs, u_hat, k1, k2, k3, absk2, nu):
+    """Per retained mode: b = i k.B_hat, L = (I - k k^T/|k|^2) b, dudt = -L + nu u_hat,
+    zero at |k| = 0 (incompressible_euler_functions.hpp:73-112, incompressible_euler.hpp:283-347).
+    Bs holds the six products at the retained modes in the reference's order
+    (B11, B21, B22, B31, B32, B33); the wavenumber arrays broadcast against them."""
+    B11, B21, B22, B31, B32, B33 = (Bs[c] for c in range(6))
+    b1 = 1j * k1 * B11 + 1j * k2 * B21 + 1j * k3 * B31
+    b2 = 1j * k1 * B21 + 1j * k2 * B22 + 1j * k3 * B32
+    b3 = 1j * k1 * B31 + 1j * k2 * B32 + 1j * k3 * B33
+    with np.errstate(divide="ignore", invalid="ignore"):
+        inv = 1.0 / absk2
+        k11, k12, k13 = k1 * k1 * inv, k1 * k2 * inv, k1 * k3 * inv
+        k22, k23, k33 = k2 * k2 * inv, k2 * k3 * inv, k3 * k3 * inv
+        L = [(1.0 - k11) * b1 + (0.0 - k12) * b2 + (0.0 - k13) * b3,
+             (0.0 - k12) * b1 + (1.0 - k22) * b2 + (0.0 - k23) * b3,
+             (0.0 - k13) * b1 + (0.0 - k23) * b2 + (1.0 - k33) * b3]
+        zero = absk2 == 0
+        out = np.empty(u_hat.shape, dtype=np.complex128)
+        for c in range(3):
+            out[c] = np.where(zero, 0.0, -L[c] + nu * u_hat[c])
+    return out
 
 
 def axpby(a, x, b, y):

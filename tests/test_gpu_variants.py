@@ -70,8 +70,35 @@ def test_dudt_every_variant(prec, dim, N, cols, rows, epi):
 
 
 @pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("dim,N,M", [(2, 32, 48), (2, 64, 96), (2, 128, 192), (2, 256, 384), (3, 16, 24),
+                                     (3, 32, 48), (3, 64, 96), (3, 34, 384), (2, 34, 768)])
+@pytest.mark.parametrize("rows", [4, 5, 6, 7])
+def test_dudt_fused_product_variants(prec, dim, N, M, rows):
+    """The fused product pass (bit 2 of the contiguous-axis variant: products
+    formed in the forward transform's loads, one work area, gap rows, input
+    pair stride, twiddles from powers of two; bit 0 the forward plan, bit 1
+    the inverse plan) against the oracle, on both plans of both transforms
+    and on heavy padding (M = 384 and 768 with few retained rows)."""
+    og = ora.Grid(dim, N, M)
+    g = az.Grid(dim, N, M)
+    oeq = ora.IncompressibleEuler(og, ora.make_viscosity(VISC_CFGS["smooth"], og))
+    u_hat = random_field_hat(dim, N, seed=900 + 10 * dim + N)
+    ref = oeq.dudt(u_hat)
+    with _Variants(prec, M, dim, 0, rows, 0):
+        eq = az.IncompressibleEuler(g, az.make_viscosity(VISC_CFGS["smooth"], g), prec)
+        d_u = to_dev(u_hat, prec)
+        d_out = torch.empty_like(d_u)
+        eq.dudt(d_out, d_u, 0.0, 0.0, 0.2)
+        got = to_host(d_out)
+        dt = eq.dt(0.2)
+    assert rel_l2(got, ref) <= TOL[prec]
+    rel_dt = 1e-13 if prec == "f64" else 1e-6
+    assert abs(dt - oeq.dt(0.2)) <= rel_dt * oeq.dt(0.2)
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
 @pytest.mark.parametrize("dim,N,B", [(2, 32, 7), (3, 16, 3)])
-@pytest.mark.parametrize("rows", [2, 3])
+@pytest.mark.parametrize("rows", [2, 3, 5, 7])
 def test_bulk_copy_kernel_batch_members_match_single(prec, dim, N, B, rows):
     """With the bulk-copy kernel, each member of a batch equals the same solve
     alone, bit for bit, over a short simulate_until.  Members have different

@@ -231,3 +231,21 @@ def test_oracle_reproduces_golden(fname):
             assert ora.rel_l2(fresh[key], data[key]) <= 1e-13, key
         else:
             np.testing.assert_array_equal(fresh[key], data[key])
+
+
+# --- the bounded-memory right-hand side (used for 3-D N = 512) ---------------
+
+@pytest.mark.parametrize("N,M,visc", [(16, 24, "Smooth Cutoff"), (24, 36, "Step"), (32, 48, "Quadratic"),
+                                      (16, 32, "Smooth Cutoff"), (64, 96, "Smooth Cutoff")])
+def test_dudt_slabs_equals_dudt(N, M, visc):
+    """dudt_slabs evaluates the same right-hand side slab by slab: equal to
+    dudt() up to rounding, and the same u_max_ (so the same dt)."""
+    rng = np.random.default_rng(N + M)
+    u_hat = ora.leray(ora.fft_forward(rng.standard_normal((3, N, N, N))))
+    g = ora.Grid(3, N, M)
+    eq = ora.IncompressibleEuler(g, ora.make_viscosity({"type": visc, "eps": 0.05}, g))
+    ref = eq.dudt(u_hat)
+    umax = eq.u_max_
+    got = eq.dudt_slabs(u_hat, xchunk=7, zchunk=5, colchunk=1000)
+    assert ora.rel_l2(got, ref) <= 1e-14
+    assert eq.u_max_ == umax

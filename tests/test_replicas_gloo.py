@@ -86,3 +86,21 @@ def test_two_gloo_ranks():
     assert max(locals_) - min(locals_) <= max(costs)
     # whole-job rate: every rank's members over the slowest rank's time
     assert out[0][5] == pytest.approx(world * len(out[0][1]) / (max(locals_) / 1e3))
+
+
+def test_bench_launches_one_rank_per_gpu_dry_run():
+    """bench.py --gpus 2 without a launcher starts two ranks itself
+    (torch.distributed.run, rendezvous on 127.0.0.1); --dry-run does the rank
+    bookkeeping on gloo without a GPU."""
+    import json
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = {k: v for k, v in os.environ.items() if k not in ("WORLD_SIZE", "RANK", "LOCAL_RANK")}
+    res = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--gpus", "2", "--dry-run"],
+                         capture_output=True, text=True, timeout=300, env=env, cwd=root)
+    assert res.returncode == 0, res.stderr[-2000:]
+    line = [ln for ln in res.stdout.splitlines() if ln.startswith("{")][-1]
+    out = json.loads(line)
+    assert out["n_gpus"] == 2 and out["ranks_seen"] == 2 and out["max_over_ranks"] == 2.0
+    assert sorted(sum(out["members"], [])) == list(range(8))
