@@ -37,6 +37,8 @@ EXPORTS = [
     "az_sim_member_start", "az_sim_member_stop", "az_group_create", "az_group_destroy",
     "az_group_steps", "az_group_steps_active", "az_group_set_end", "az_group_simulate_until",
     "az_debug_set_wait_limit", "az_debug_get_wait_limit", "az_euler_noalloc_status",
+    "az_init_physical", "az_init_envelope", "az_init_normalize_energy", "az_random_uniform",
+    "az_philox4x32_10", "az_bench_radix16_stage",
 ]
 
 
@@ -56,6 +58,16 @@ class az_visc(ct.Structure):
 class az_euler_desc(ct.Structure):
     _fields_ = [("dim", ct.c_int), ("N_phys", ct.c_longlong), ("N_phys_pad", ct.c_longlong),
                 ("precision", ct.c_int), ("visc", az_visc), ("batch", ct.c_int)]
+
+
+AZ_INIT_TAYLOR_GREEN, AZ_INIT_TAYLOR_GREEN_WORKLOAD, AZ_INIT_DOUBLE_SHEAR_LAYER, AZ_INIT_GAUSSIAN_NOISE = 0, 1, 2, 3
+
+
+class az_init_desc(ct.Structure):
+    _fields_ = [("kind", ct.c_int), ("dim", ct.c_int), ("N", ct.c_longlong), ("precision", ct.c_int),
+                ("batch", ct.c_int), ("rho", ct.c_double), ("delta", ct.c_double),
+                ("deltas", ct.POINTER(ct.c_double)), ("phases", ct.POINTER(ct.c_double)),
+                ("seed", ct.c_ulonglong), ("member0", ct.c_longlong)]
 
 
 class az_fft_desc(ct.Structure):
@@ -113,6 +125,12 @@ def _load():
         "az_debug_set_wait_limit": (I, [I]),
         "az_debug_get_wait_limit": (I, []),
         "az_euler_noalloc_status": (I, [P]),
+        "az_init_physical": (I, [ct.POINTER(az_init_desc), P, P]),
+        "az_init_envelope": (I, [I, LL, I, P, I, D, P]),
+        "az_init_normalize_energy": (I, [I, LL, I, P, I, D, P]),
+        "az_random_uniform": (I, [ct.c_ulonglong, ct.c_ulonglong, ct.c_ulonglong, ct.POINTER(D)]),
+        "az_philox4x32_10": (I, [ct.POINTER(ct.c_uint), ct.POINTER(ct.c_uint), ct.POINTER(ct.c_uint)]),
+        "az_bench_radix16_stage": (I, [I, I, ct.POINTER(D), ct.POINTER(D)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -100,29 +100,39 @@ __global__ void k_diag_final(const double* parts, double scale, double* out) {
   out[2 * b + 1] = 0.5 * scale * W.value();
 }
 
+// Partials and per-member (energy, enstrophy) of `batch` members of u_hat
+// [batch][dim][N]([N])[N/2+1]; buf holds kDiagDoublesPerMember per member:
+// the partial sums, then the results at buf + batch * kDiagParts * 2.
+cudaError_t diag_launch(int dim, int precision, long long N, const void* u_hat, int batch, double* buf,
+                        cudaStream_t st) {
+  const long long nh = N / 2 + 1;
+  const long long plane = (dim == 2 ? N : N * N) * nh;
+  const long long member = dim * plane;
+  double* parts = buf;
+  double* res = parts + size_t(batch) * kDiagParts * 2;
+  const dim3 grid(kDiagParts, unsigned(batch));
+  if (precision == AZ_PREC_F64) {
+    if (dim == 2) k_diag_partials<double, 2><<<grid, kDiagThreads, 0, st>>>((const double2*)u_hat, N, nh, plane, member, parts);
+    else k_diag_partials<double, 3><<<grid, kDiagThreads, 0, st>>>((const double2*)u_hat, N, nh, plane, member, parts);
+  } else {
+    if (dim == 2) k_diag_partials<float, 2><<<grid, kDiagThreads, 0, st>>>((const float2*)u_hat, N, nh, plane, member, parts);
+    else k_diag_partials<float, 3><<<grid, kDiagThreads, 0, st>>>((const float2*)u_hat, N, nh, plane, member, parts);
+  }
+  const double Nd = dim == 2 ? double(N) * N : double(N) * N * N;
+  k_diag_final<<<unsigned(batch), 32, 0, st>>>(parts, 1.0 / (Nd * Nd), res);
+  return cudaGetLastError();
+}
+
 }  // namespace azb
 
 using namespace azb;
 
 az_status az_euler_diagnostics(az_euler e, const void* u_hat, void* stream, double* energy, double* enstrophy) {
   if (!e || !u_hat) return set_error(AZ_ERR_INVALID, "az_euler_diagnostics: null argument");
-  const long long N = e->N, nh = e->Nh;
-  const long long plane = (e->dim == 2 ? N : N * N) * nh;
   static_assert(kDiagParts * 2 + 2 == kDiagDoublesPerMember, "diagnostics buffer layout");
-  double* parts = e->diag;
-  double* res = parts + size_t(e->batch) * kDiagParts * 2;
+  double* res = e->diag + size_t(e->batch) * kDiagParts * 2;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  const dim3 grid(kDiagParts, unsigned(e->batch));
-  if (e->prec == AZ_PREC_F64) {
-    if (e->dim == 2) k_diag_partials<double, 2><<<grid, kDiagThreads, 0, st>>>((const double2*)u_hat, N, nh, plane, e->state_mem, parts);
-    else k_diag_partials<double, 3><<<grid, kDiagThreads, 0, st>>>((const double2*)u_hat, N, nh, plane, e->state_mem, parts);
-  } else {
-    if (e->dim == 2) k_diag_partials<float, 2><<<grid, kDiagThreads, 0, st>>>((const float2*)u_hat, N, nh, plane, e->state_mem, parts);
-    else k_diag_partials<float, 3><<<grid, kDiagThreads, 0, st>>>((const float2*)u_hat, N, nh, plane, e->state_mem, parts);
-  }
-  const double Nd = e->dim == 2 ? double(N) * N : double(N) * N * N;
-  k_diag_final<<<unsigned(e->batch), 32, 0, st>>>(parts, 1.0 / (Nd * Nd), res);
-  cudaError_t ce = cudaGetLastError();
+  cudaError_t ce = diag_launch(e->dim, e->prec, e->N, u_hat, e->batch, e->diag, st);
   if (ce != cudaSuccess) return set_error(AZ_ERR_CUDA, cudaGetErrorString(ce));
   std::vector<double> h(size_t(e->batch) * 2);
   ce = cudaMemcpyAsync(h.data(), res, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st);

@@ -317,66 +317,16 @@ template <int... Rs> struct RadixInfo<Radices<Rs...>> {
 };
 
 // ---------------------------------------------------------------------------
-// Shared-memory row layouts of a transform's columns: element (row, col) of
-// the exchange buffer sits at at(row, col).
-//   Rows<SROW>    plain rows of SROW elements;
-//   Rows16<SROW>  one gap row after every 16 rows, so rows 16 apart (the
-//                 first stage's stores of a radix-16 stage, rows b*16 + r
-//                 for consecutive butterflies b) fall on different banks.
-// ---------------------------------------------------------------------------
-template <int SROW> struct Rows {
-  static constexpr int nrows(int L) { return L; }
-  static __device__ __forceinline__ int at(int row, int col) { return row * SROW + col; }
-};
-template <int SROW> struct Rows16 {
-  static constexpr int nrows(int L) { return L + (L + 15) / 16; }
-  static __device__ __forceinline__ int at(int row, int col) { return (row + (row >> 4)) * SROW + col; }
-};
-
-// Twiddle schemes of a stage of radix R (the factors W_L^{r step}, r in [1, R)):
-//   TW_LOAD   every factor read from the table;
-//   TW_POW2   the factors at powers of two r read from the table, the others
-//             formed as w_r = w_h * w_{r-h} (h the highest power of two below
-//             r): one complex multiplication instead of one shared-memory
-//             load each.  For R = 24: 5 loads and 18 multiplications instead
-//             of 23 loads; each formed factor carries at most three more
-//             roundings than a table entry.
-enum TwScheme : int { TW_LOAD = 0, TW_POW2 = 1 };
-
-constexpr int pow2_at_most(int x) {
-  int p = 1;
-  while (p * 2 <= x) p *= 2;
-  return p;
-}
-
-template <int R, int I> struct TwPow2 {
-  template <typename C>
-  static __device__ __forceinline__ void form(C (&w)[R], const C* tw, int step) {
-    if constexpr (I < R) {
-      constexpr int h = pow2_at_most(I);
-      if constexpr (h == I) {
-        w[I] = tw[I * step];
-      } else {
-        w[I] = cmul(w[h], w[I - h]);
-      }
-      TwPow2<R, I + 1>::form(w, tw, step);
-    }
-  }
-};
-
-// ---------------------------------------------------------------------------
 // The stage engine.
 //   C      complex vector type (float2 / double2)
 //   S      -1 forward, +1 inverse
 //   L, E   length and elements per thread
 //   SROW   shared-memory row stride in elements
-//   Lay    row layout (Rows<SROW> unless given)
-//   TWM    twiddle scheme (TwScheme)
 // Thread (col, tl): tl in [0, L/E).  v[q*R + r] is element r of butterfly
 // b = tl + q*(L/E) of the current stage.
 // tw: table of W_L^m = exp(-2 pi i m / L), m in [0, L), in shared memory.
 // ---------------------------------------------------------------------------
-template <typename C, int S, int L, int E, int SROW, typename Lay = Rows<SROW>, int TWM = TW_LOAD>
+template <typename C, int S, int L, int E, int SROW>
 struct Engine {
   static constexpr int TPL = L / E;
 
@@ -397,18 +347,10 @@ struct Engine {
         const int b = tl + q * TPL;
         const int j = b % NS;
         const int step = j * (L / (NS * R));
-        if constexpr (TWM == TW_POW2 && R > 4) {
-          C w[R];
-          TwPow2<R, 1>::form(w, tw, step);
 #pragma unroll
-          for (int r = 1; r < R; ++r)
-            v[q * R + r] = (S < 0) ? cmul(v[q * R + r], w[r]) : cmulc(v[q * R + r], w[r]);
-        } else {
-#pragma unroll
-          for (int r = 1; r < R; ++r) {
-            const C w = tw[r * step];
-            v[q * R + r] = (S < 0) ? cmul(v[q * R + r], w) : cmulc(v[q * R + r], w);
-          }
+        for (int r = 1; r < R; ++r) {
+          const C w = tw[r * step];
+          v[q * R + r] = (S < 0) ? cmul(v[q * R + r], w) : cmulc(v[q * R + r], w);
         }
       }
       DFT<R, S, C>::run(&v[q * R]);
@@ -424,7 +366,7 @@ struct Engine {
       const int b = tl + q * TPL;
       const int base = (b / NS) * NS * R + (b % NS);
 #pragma unroll
-      for (int r = 0; r < R; ++r) sm[Lay::at(base + r * NS, col)] = v[q * R + r];
+      for (int r = 0; r < R; ++r) sm[(base + r * NS) * SROW + col] = v[q * R + r];
     }
   }
 
@@ -434,7 +376,7 @@ struct Engine {
     for (int q = 0; q < E / R; ++q) {
       const int b = tl + q * TPL;
 #pragma unroll
-      for (int r = 0; r < R; ++r) v[q * R + r] = sm[Lay::at(b + r * (L / R), col)];
+      for (int r = 0; r < R; ++r) v[q * R + r] = sm[(b + r * (L / R)) * SROW + col];
     }
   }
 
@@ -485,24 +427,6 @@ __device__ __forceinline__ void fft_run(C* sm, C (&v)[P::E], const C* tw, int co
                                         bool active = true) {
   using Info = RadixInfo<typename P::R>;
   using Eng = Engine<C, S, L, P::E, SROW>;
-  Eng::template run<1>(sm, v, col, tl, tw, active, typename P::R{});
-  if constexpr (SYNC_STORE) __syncthreads();
-  if (!active) return;
-#pragma unroll
-  for (int q = 0; q < P::E / Info::last; ++q) {
-#pragma unroll
-    for (int r = 0; r < Info::last; ++r) {
-      store(Eng::template out_row<Info::last>(tl, q, r), v[q * Info::last + r]);
-    }
-  }
-}
-
-// fft_run with a row layout and a twiddle scheme (see Rows16, TwScheme).
-template <typename C, int S, int L, typename Lay, int TWM, bool SYNC_STORE, typename P, typename Store>
-__device__ __forceinline__ void fft_run_lay(C* sm, C (&v)[P::E], const C* tw, int col, int tl, Store&& store,
-                                            bool active = true) {
-  using Info = RadixInfo<typename P::R>;
-  using Eng = Engine<C, S, L, P::E, 1, Lay, TWM>;
   Eng::template run<1>(sm, v, col, tl, tw, active, typename P::R{});
   if constexpr (SYNC_STORE) __syncthreads();
   if (!active) return;

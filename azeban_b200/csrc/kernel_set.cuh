@@ -57,14 +57,13 @@ template <typename T, int L, int V> struct Tiles {
   static constexpr int NLPR = kclamp(kpow2floor(49152 / (L * CB)), 1, 64);
 };
 
-// Line pairs per chunk of k_zfused: a work area (gap rows included) of about
-// 80 KB, raised until the CTA's thread count is a whole number of warps.
+// Line pairs per chunk of k_zfused: a work area of about 80 KB, raised until
+// the CTA's thread count is a whole number of warps.
 template <typename T, int L, int DIM, int VF> struct ZFTile {
   static constexpr int CB = int(sizeof(cvec<T>));
   static constexpr int NB = DIM * (DIM + 1) / 2;
   static constexpr int TPL = Plan<L, VF>::TPL;
-  static constexpr int ROWS = Rows16<1>::nrows(L);
-  static constexpr int BUDGET = kclamp(kpow2floor(81920 / (ROWS * NB * CB)), 1, 16);
+  static constexpr int BUDGET = kclamp(kpow2floor(81920 / (L * NB * CB)), 1, 16);
   static constexpr int G = (TPL % 32 == 0) ? 32 : (TPL % 16 == 0) ? 16 : (TPL % 8 == 0) ? 8
                          : (TPL % 4 == 0) ? 4 : (TPL % 2 == 0) ? 2 : 1;  // gcd(TPL, 32)
   static constexpr int MIN = DIM == 3 ? (G >= 16 ? 1 : 16 / G) : 32 / G;

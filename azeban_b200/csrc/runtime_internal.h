@@ -42,6 +42,14 @@ struct az_euler_s {
 // Doubles of az_euler_s::diag per member.
 constexpr int kDiagDoublesPerMember = 512 * 2 + 2;
 
+namespace azb {
+// Energy and enstrophy partial sums and results of `batch` members of u_hat
+// [batch][dim][N]([N])[N/2+1] into buf (kDiagDoublesPerMember per member;
+// the (energy, enstrophy) pairs at buf + batch * (kDiagDoublesPerMember - 2)).
+cudaError_t diag_launch(int dim, int precision, long long N, const void* u_hat, int batch, double* buf,
+                        cudaStream_t st);
+}  // namespace azb
+
 
 namespace azb {
 // Sizes, member strides, padded row strides, normalisation and M^d of an

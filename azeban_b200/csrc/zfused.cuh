@@ -12,15 +12,11 @@
 //  - input, velocity and product columns share one region (each phase reads
 //    its inputs into registers before the barrier that precedes its first
 //    store), so a CTA needs one work area instead of two;
-//  - the exchange buffers have a gap row after every 16 rows (Rows16): the
-//    stores of a radix-16 first stage no longer collide on banks;
 //  - each input line pair lands at a stride chosen on the host so that the
 //    inverse transform's first-stage reads (the half spectra, Hermitian
 //    extension folded in) fall on different banks, and the inverse
 //    transform's threads take 16 column slots per row group when the CTA
-//    has the threads, so a half-warp reads one row group;
-//  - stages of radix above 4 form their twiddle factors from the table
-//    entries at powers of two (TW_POW2).
+//    has the threads, so a half-warp reads one row group.
 // The mbarrier wait for the bulk copies is bounded as in k_zpass.
 //
 // Reference: the inverse transform, max_norm and computeB of
@@ -63,11 +59,8 @@ template <typename T, int L, int NLP, int DIM, int VF, int VI> struct ZFShape {
   static constexpr int CS = (NINV <= 16 && 16 * PI::TPL <= NT) ? 16
                             : (NINV <= 8 && 8 * PI::TPL <= NT) ? 8 : NINV;
   static_assert(CS * PI::TPL <= NT, "the inverse transform needs CS * TPL threads");
-  using LayV = Rows16<NINV>;
-  using LayP = Rows16<NFWD>;
-  static constexpr int ROWS = Rows16<1>::nrows(L);
-  static constexpr long long V_ELEMS = (long long)ROWS * NINV;
-  static constexpr long long P_ELEMS = (long long)ROWS * NFWD;
+  static constexpr long long V_ELEMS = (long long)L * NINV;
+  static constexpr long long P_ELEMS = (long long)L * NFWD;
   // FP32: a register cap for 12 resident warps per SM; FP64 plans need theirs.
   static constexpr int MINB = CB == 8 ? (NT >= 384 ? 1 : 384 / NT) : 1;
   static constexpr int OFF_TW = 16;
@@ -87,8 +80,6 @@ __global__ void __launch_bounds__(ZFShape<T, L, NLP, DIM, VF, VI>::NT, ZFShape<T
   using Z = ZFShape<T, L, NLP, DIM, VF, VI>;
   using PI = typename Z::PI;
   using PF = typename Z::PF;
-  using LayV = typename Z::LayV;
-  using LayP = typename Z::LayP;
   constexpr int NB = Z::NB;
   constexpr int NINV = Z::NINV;
   constexpr int NFWD = Z::NFWD;
@@ -164,13 +155,13 @@ __global__ void __launch_bounds__(ZFShape<T, L, NLP, DIM, VF, VI>::NT, ZFShape<T
     };
     C v[PI::E];
     fft_load<C, L, PI>(v, tl, load, active);
-    fft_run_lay<C, +1, L, LayV, TW_POW2, true, PI>(
+    fft_run<C, +1, L, NINV, true, PI>(
         w, v, tw, col, tl,
         [&](int m, C x) {
           const typename AB::U bx = AB::of(x.x), by = AB::of(x.y);
           vbits = bx > vbits ? bx : vbits;
           vbits = by > vbits ? by : vbits;
-          w[LayV::at(m, col)] = cmk<C>(x.x * norm, x.y * norm);
+          w[m * NINV + col] = cmk<C>(x.x * norm, x.y * norm);
         },
         active);
   }
@@ -187,14 +178,13 @@ __global__ void __launch_bounds__(ZFShape<T, L, NLP, DIM, VF, VI>::NT, ZFShape<T
     const int ci = p * DIM + prod_i<DIM>(c);
     const int cj = p * DIM + prod_j<DIM>(c);
     auto load = [&](int m) {
-      const C x = w[LayV::at(m, ci)];
-      const C y = w[LayV::at(m, cj)];
+      const C x = w[m * NINV + ci];
+      const C y = w[m * NINV + cj];
       return cmk<C>(x.x * y.x, x.y * y.y);
     };
     C v[PF::E];
     fft_load<C, L, PF>(v, tl, load);
-    fft_run_lay<C, -1, L, LayP, TW_POW2, true, PF>(w, v, tw, col, tl,
-                                                   [&](int m, C x) { w[LayP::at(m, col)] = x; });
+    fft_run<C, -1, L, NFWD, true, PF>(w, v, tw, col, tl, [&](int m, C x) { w[m * NFWD + col] = x; });
   }
   __syncthreads();
 
@@ -209,8 +199,8 @@ __global__ void __launch_bounds__(ZFShape<T, L, NLP, DIM, VF, VI>::NT, ZFShape<T
     for (int r = tid; r < nb_nh; r += NT) {
       const int kb = r / NB;
       const int cf = p * NB + (r - kb * NB);
-      const C x = w[LayP::at(kb, cf)];
-      const C y = w[LayP::at(kb == 0 ? 0 : L - kb, cf)];
+      const C x = w[kb * NFWD + cf];
+      const C y = w[(kb == 0 ? 0 : L - kb) * NFWD + cf];
       oa[r] = cmk<C>(T(0.5) * (x.x + y.x), T(0.5) * (x.y - y.y));
       ob[r] = cmk<C>(T(0.5) * (x.y + y.y), T(-0.5) * (x.x - y.x));
     }

@@ -1,32 +1,63 @@
-"""Initial data for the benchmark workloads, built on the device.
+"""Initial data for the workloads and the reference's initialisers, built on
+the device.
 
-Each generator samples a physical field at x_i = 2 pi i / N (the reference's
-sampling, src/azeban/init/taylor_green.cpp:40-41), transforms it with this
+Each generator samples its physical field in one kernel of the library
+(az_init_physical, straight into a device array), transforms it with the
 library's FFT and Leray-projects it, as Initializer::initialize does
-(include/azeban/init/initializer.hpp:68-75).
+(include/azeban/init/initializer.hpp:68-75).  Random values (shear-layer
+phases, Gaussian coefficients) come from the library's counter-based Philox
+stream (seed, member), so a member's field depends only on its seed and
+member index, not on the batch it is generated in.
 """
 
 from __future__ import annotations
 
+import ctypes as ct
 import math
 
 import torch
 
-from .core import FFT, FFT_FORWARD, leray
+from . import _lib
+from ._lib import check, lib
+from .core import FFT, FFT_FORWARD, _stream_ptr, leray, precision_code
 
-_RDT = {"f64": torch.float64, "f32": torch.float32}
-_CDT = {"f64": torch.complex128, "f32": torch.complex64}
-
-
-def _coords(N, dim, dtype):
-    x = (2 * math.pi / N) * torch.arange(N, device="cuda", dtype=torch.float64)
-    return [g.to(dtype) for g in torch.meshgrid(*([x] * dim), indexing="ij")]
+_RDT = {0: torch.float64, 1: torch.float32}
 
 
-def spectral(u_phys: torch.Tensor, project: bool = True) -> torch.Tensor:
-    """Forward transform of a [(B,) dim, N, ...] physical field (+ Leray)."""
+def physical(kind: int, dim: int, N: int, precision="f64", batch: int = 1, rho: float = 0.0,
+             delta: float = 0.0, deltas=None, phases=None, seed: int = 0, member0: int = 0,
+             stream=None) -> torch.Tensor:
+    """The physical field [batch, dim, N, ...] of one generator (az_init_physical)."""
+    prec = precision_code(precision)
+    u = torch.empty((batch, dim) + (N,) * dim, dtype=_RDT[prec], device="cuda")
+    keep = []
+
+    def arr(x, n):
+        if x is None:
+            return None
+        flat = [float(v) for v in x]
+        if len(flat) != n:
+            raise ValueError(f"expected {n} values, got {len(flat)}")
+        a = (ct.c_double * n)(*flat)
+        keep.append(a)
+        return ct.cast(a, ct.POINTER(ct.c_double))
+
+    nd = 8 if dim == 2 else 24
+    desc = _lib.az_init_desc(kind, dim, N, prec, batch, float(rho), float(delta),
+                             arr(None if deltas is None else [v for row in deltas for v in row], batch * nd),
+                             arr(phases, batch), int(seed) & (2**64 - 1), int(member0))
+    check(lib.az_init_physical(ct.byref(desc), u.data_ptr(), _stream_ptr(stream)))
+    return u
+
+
+def spectral(u_phys: torch.Tensor, project: bool = True, batched: bool | None = None) -> torch.Tensor:
+    """Forward transform of a [(B,) dim, N, ...] physical field (+ Leray).
+    batched: whether axis 0 is the member axis (None: inferred from the rank,
+    which cannot tell a batch of three 2-D fields from one 3-D field)."""
     # [dim, N...] (one member) or [B, dim, N...]
-    if u_phys.dim() >= 3 and u_phys.shape[0] in (2, 3) and u_phys.dim() == u_phys.shape[0] + 1:
+    if batched is None:
+        batched = not (u_phys.dim() >= 3 and u_phys.shape[0] in (2, 3) and u_phys.dim() == u_phys.shape[0] + 1)
+    if not batched:
         flat = u_phys.unsqueeze(0)
         squeeze = True
     else:
@@ -48,58 +79,61 @@ def spectral(u_phys: torch.Tensor, project: bool = True) -> torch.Tensor:
 def taylor_green(dim: int, N: int, precision: str = "f64") -> torch.Tensor:
     """Taylor-Green of the workloads: (sin x cos y, -cos x sin y) in 2-D and
     (sin x cos y cos z, -cos x sin y cos z, 0) in 3-D; spectral, [dim, N, ..., N/2+1]."""
-    dt = torch.float64
-    if dim == 2:
-        x, y = _coords(N, 2, dt)
-        u = torch.stack([torch.sin(x) * torch.cos(y), -torch.cos(x) * torch.sin(y)])
-    else:
-        x, y, z = _coords(N, 3, dt)
-        u = torch.stack([torch.sin(x) * torch.cos(y) * torch.cos(z),
-                         -torch.cos(x) * torch.sin(y) * torch.cos(z),
-                         torch.zeros_like(x)])
-    return spectral(u.to(_RDT[precision]))
+    return spectral(physical(_lib.AZ_INIT_TAYLOR_GREEN_WORKLOAD, dim, N, precision), batched=True)[0]
 
 
-def double_shear_layer(N: int, rho: float, delta: float, phases, precision: str = "f64") -> torch.Tensor:
+def taylor_green_reference(dim: int, N: int, precision: str = "f64", deltas=None) -> torch.Tensor:
+    """The reference's Taylor-Green (src/azeban/init/taylor_green.cpp:29-46,
+    :146-184): (cos x sin y, -sin x cos y) in 2-D, (cos x sin y sin z,
+    -sin x cos y sin z, 0) in 3-D, plus the perturbation modes with amplitudes
+    deltas [batch][8 or 24] (the reference's draws, already divided by 4 or
+    8); spectral, [batch, dim, N, ..., N/2+1] (batch 1 without deltas)."""
+    batch = 1 if deltas is None else len(deltas)
+    return spectral(physical(_lib.AZ_INIT_TAYLOR_GREEN, dim, N, precision, batch, deltas=deltas), batched=True)
+
+
+def double_shear_layer(N: int, rho: float, delta: float, phases=None, precision: str = "f64", seed: int = 0,
+                       member0: int = 0, batch: int | None = None) -> torch.Tensor:
     """Double shear layer (src/azeban/init/double_shear_layer.cpp:25-43) with a
     phase per member: u = tanh(2 pi (y - 1/4)/rho) for y < 1/2, else
-    tanh(2 pi (3/4 - y)/rho); v = delta sin(2 pi x + phi).  [B, 2, N, N/2+1]."""
-    i = torch.arange(N, device="cuda", dtype=torch.float64) / N
-    x = i[:, None].expand(N, N)
-    y = i[None, :].expand(N, N)
-    if rho == 0:
-        u = torch.where((y - 0.5).abs() < 0.25, 1.0, -1.0)
-    else:
-        u = torch.where(y < 0.5, torch.tanh(2 * math.pi * (y - 0.25) / rho),
-                        torch.tanh(2 * math.pi * (0.75 - y) / rho))
-    ph = torch.as_tensor(list(phases), device="cuda", dtype=torch.float64)
-    v = delta * torch.sin(2 * math.pi * x[None] + ph[:, None, None])
-    field = torch.stack([u[None].expand_as(v), v], dim=1)
-    return spectral(field.to(_RDT[precision]).contiguous())
+    tanh(2 pi (3/4 - y)/rho); v = delta sin(2 pi x + phi).  phases: given per
+    member, or None to draw phi ~ U[0, 2 pi) from stream (seed, member0 + b)
+    for `batch` members.  [B, 2, N, N/2+1]."""
+    if phases is not None:
+        batch = len(phases)
+    elif batch is None:
+        batch = 1
+    return spectral(physical(_lib.AZ_INIT_DOUBLE_SHEAR_LAYER, 2, N, precision, batch, rho=rho, delta=delta,
+                             phases=phases, seed=seed, member0=member0), batched=True)
 
 
-def fractional_brownian(dim: int, N: int, hurst: float = 0.75, seed: int = 0, precision: str = "f64") -> torch.Tensor:
+def stream_uniform(seed: int, member: int, index: int = 0) -> float:
+    """Value `index` of random stream (seed, member) as a uniform in [0, 1)."""
+    out = ct.c_double()
+    check(lib.az_random_uniform(int(seed) & (2**64 - 1), int(member), int(index), ct.byref(out)))
+    return out.value
+
+
+def shear_layer_phase(seed: int, member: int = 0) -> float:
+    """The phase az_init_physical draws for member `member` of seed `seed`."""
+    return 2 * math.pi * stream_uniform(seed, member, 0)
+
+
+def fractional_brownian(dim: int, N: int, hurst: float = 0.75, seed: int = 0, precision: str = "f64",
+                        batch: int = 1, member0: int = 0) -> torch.Tensor:
     """Random divergence-free field: Gaussian Fourier coefficients with
     amplitude |n|^-(H + d/2), Leray-projected, normalised to kinetic energy
-    1/2 <|u|^2> = 1.  The coefficients come from the forward transform of
-    seeded Gaussian white noise, so the spectrum is Hermitian-consistent.
-    [dim, N, ..., N/2+1].  (azeban's own BrownianMotion,
+    1/2 <|u|^2> = 1.  The coefficients are the forward transform of seeded
+    Gaussian white noise (stream (seed, member0 + b)), so the spectrum is
+    Hermitian-consistent.  [dim, N, ..., N/2+1] for batch 1, else
+    [batch, dim, ...].  (azeban's own BrownianMotion,
     src/azeban/init/brownian_motion.cpp:144-203, draws uniform coefficients;
     this is the Gaussian form of the workloads.)"""
-    gen = torch.Generator(device="cuda").manual_seed(int(seed))
-    noise = torch.randn((dim,) + (N,) * dim, generator=gen, device="cuda", dtype=torch.float64)
-    u_hat = spectral(noise.to(_RDT[precision]), project=False)
-    idx = torch.arange(N, device="cuda", dtype=torch.float64)
-    signed = torch.where(idx >= N // 2 + 1, idx - N, idx)
-    axes = [signed] * (dim - 1) + [torch.arange(N // 2 + 1, device="cuda", dtype=torch.float64)]
-    k2 = sum(g * g for g in torch.meshgrid(*axes, indexing="ij"))
-    amp = torch.where(k2 > 0, k2.clamp_min(1e-300) ** (-(hurst + dim / 2.0) / 2.0), torch.zeros_like(k2))
-    u_hat = u_hat * amp.to(u_hat.real.dtype)
+    prec = precision_code(precision)
+    noise = physical(_lib.AZ_INIT_GAUSSIAN_NOISE, dim, N, precision, batch, seed=seed, member0=member0)
+    u_hat = spectral(noise, project=False, batched=True).contiguous()
+    check(lib.az_init_envelope(dim, N, prec, u_hat.data_ptr(), batch, -(hurst + dim / 2.0),
+                               _stream_ptr(None)))
     leray(u_hat)
-    # kinetic energy of the unnormalised half spectrum (Parseval)
-    w = torch.full((N // 2 + 1,), 2.0, device="cuda", dtype=torch.float64)
-    w[0] = 1.0
-    if N % 2 == 0:
-        w[N // 2] = 1.0
-    e = 0.5 * (w * (u_hat.abs().to(torch.float64) ** 2)).sum() / float(N) ** (2 * dim)
-    return (u_hat / torch.sqrt(e).to(u_hat.real.dtype)).contiguous()
+    check(lib.az_init_normalize_energy(dim, N, prec, u_hat.data_ptr(), batch, 1.0, _stream_ptr(None)))
+    return u_hat[0] if batch == 1 else u_hat

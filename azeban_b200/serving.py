@@ -126,8 +126,8 @@ def poisson_stream(rate: float, duration: float, seed: int = 0, classes=CLASSES,
 def initial_state(req: Request, precision: str):
     """The request's initial spectral state, generated on the device."""
     if req.dim == 2:
-        phase = float(np.random.default_rng(req.seed).uniform(0.0, 2 * math.pi))
-        return azinit.double_shear_layer(req.N, math.pi / 15, 0.05, [phase], precision)[0]
+        # phase ~ U[0, 2 pi) from the counter-based stream (seed, 0), drawn on the device
+        return azinit.double_shear_layer(req.N, math.pi / 15, 0.05, None, precision, seed=req.seed)[0]
     return azinit.fractional_brownian(3, req.N, 0.75, req.seed, precision)
 
 

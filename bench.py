@@ -55,7 +55,8 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workload", default="tg3d256",
-                    choices=["tg3d256", "tg2d64", "tg3d-accuracy", "dsl-ensemble", "fbm512", "serving"],
+                    choices=["tg3d256", "tg2d64", "tg3d-accuracy", "dsl-ensemble", "fbm512", "serving",
+                             "dft-gemm-stage"],
                     help="tg3d256 is the headline; the others are the remaining workloads, one JSON line each")
     ap.add_argument("--duration", type=float, default=60.0, help="serving: seconds of Poisson arrivals")
     ap.add_argument("--rate", type=float, default=200.0, help="serving: arrivals per second")
@@ -494,10 +495,26 @@ def run_tg2d64(args):
                       "l2_rel_gpu_vs_oracle": ora.rel_l2(sim.u().cpu().numpy(), osim.u_)}), flush=True)
 
 
+def _until_rounding_state(sim, group, t):
+    """simulate_until(t) of a one-member FP64 simulation, with its state
+    rounded to FP32 after every step (the rounding any FP32 state storage
+    injects once per step)."""
+    import torch
+    group.set_end(t)
+    while sim.state()[0][0] < t:
+        group.steps(1)
+        u = sim.u()
+        u.copy_(u.to(torch.complex64).to(torch.complex128))
+
+
 def run_tg3d_accuracy(args):
     """Taylor-Green 3-D at 128^3 and 256^3, FP64 and FP32 bulk: relative L2 of
     FP32 vs FP64 at 10 output times over [0, 1/(2 pi)] (t in [0, 1] on
-    [0, 2 pi)^3) and at azeban t = 1, with the FP64 rounded-initial-state floor."""
+    [0, 2 pi)^3) and at azeban t = 1, beside two floors: FP64 started from
+    the FP32-rounded initial state (the flow's sensitivity to one rounding at
+    t = 0), and FP64 with its state rounded to FP32 after every step (the
+    rounding a FP32 state stores into every step, without any FP32
+    arithmetic)."""
     import torch
 
     import azeban_b200 as az
@@ -511,7 +528,10 @@ def run_tg3d_accuracy(args):
         sims = {"fp32": az.Simulation(g, C_CFL, az.SSP_RK3(az.IncompressibleEuler(g, v, "f32")), u32),
                 "fp64": az.Simulation(g, C_CFL, az.SSP_RK3(az.IncompressibleEuler(g, v, "f64")), u64),
                 "floor": az.Simulation(g, C_CFL, az.SSP_RK3(az.IncompressibleEuler(g, v, "f64")),
-                                       u32.to(torch.complex128).contiguous())}
+                                       u32.to(torch.complex128).contiguous()),
+                "storage": az.Simulation(g, C_CFL, az.SSP_RK3(az.IncompressibleEuler(g, v, "f64")),
+                                         u32.to(torch.complex128).contiguous())}
+        storage_group = az.Group([sims["storage"]])
         times = [(i + 1) / (10 * 2 * math.pi) for i in range(10)] + [1.0]
         rows = []
         busy_ms = {"fp32": 0.0, "fp64": 0.0}
@@ -519,7 +539,10 @@ def run_tg3d_accuracy(args):
             for name, s_ in sims.items():
                 e0, e1 = _ev(), _ev()
                 e0.record()
-                s_.simulate_until(t)
+                if name == "storage":
+                    _until_rounding_state(s_, storage_group, t)
+                else:
+                    s_.simulate_until(t)
                 e1.record()
                 torch.cuda.synchronize()
                 if name in busy_ms:
@@ -527,14 +550,15 @@ def run_tg3d_accuracy(args):
             ref = sims["fp64"].u()
             nrm = torch.linalg.vector_norm(ref)
             rows.append({"t": t, "l2_fp32_vs_fp64": float(torch.linalg.vector_norm(sims["fp32"].u().to(torch.complex128) - ref) / nrm),
-                         "floor": float(torch.linalg.vector_norm(sims["floor"].u() - ref) / nrm)})
+                         "floor": float(torch.linalg.vector_norm(sims["floor"].u() - ref) / nrm),
+                         "floor_state_rounded_each_step": float(torch.linalg.vector_norm(sims["storage"].u() - ref) / nrm)})
         # one member each, stepped to t = 1 (azeban units) through simulate_until
         rate = {}
         for name, ms in busy_ms.items():
             steps = sims[name].state()[1][0]
             rate[name] = {"steps": steps, "ms_per_step": ms / steps, "member_steps_per_s": steps / (ms / 1e3)}
         out.append({"N": N, "outputs": rows, "throughput_one_member": rate})
-        del sims
+        del sims, storage_group
     print(json.dumps({"workload": "TG-3D accuracy FP32 bulk vs FP64", "results": out}), flush=True)
 
 
@@ -691,6 +715,27 @@ def run_serving(args):
           flush=True)
 
 
+def run_dft_gemm_stage(args):
+    """One radix-16 DFT stage of FP32 columns in shared memory: the transform
+    passes' butterflies against a DFT-as-GEMM stage on the tensor pipe
+    (mma.sync m16n8k8 TF32, three-term head/tail split), time per column and
+    stage on every SM and the error of one stage."""
+    import ctypes as ct
+
+    import torch
+
+    from azeban_b200 import _lib
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    res = {}
+    for name, method in (("butterfly", 0), ("gemm_3xtf32", 1)):
+        ns, err = ct.c_double(), ct.c_double()
+        _lib.check(_lib.lib.az_bench_radix16_stage(method, 8 * sms, ct.byref(ns), ct.byref(err)))
+        res[name] = {"ns_per_column_stage": ns.value, "max_rel_err": err.value}
+    res["gemm_over_butterfly_time"] = res["gemm_3xtf32"]["ns_per_column_stage"] / res["butterfly"]["ns_per_column_stage"]
+    print(json.dumps({"workload": "radix-16 DFT stage, FP32 complex columns in shared memory, "
+                                  f"{8 * sms} CTAs of 128 columns", "results": res}), flush=True)
+
+
 def launch_ranks(args):
     """--gpus N without a launcher: re-run this command under
     torch.distributed.run with N ranks on this node (one per GPU, rendezvous
@@ -735,7 +780,7 @@ def main():
         run_reference(args, rank, world)
         return
     extra = {"tg2d64": run_tg2d64, "tg3d-accuracy": run_tg3d_accuracy, "dsl-ensemble": run_dsl_ensemble,
-             "fbm512": run_fbm512, "serving": run_serving}
+             "fbm512": run_fbm512, "serving": run_serving, "dft-gemm-stage": run_dft_gemm_stage}
     if args.workload in extra:
         import torch
         torch.cuda.set_device(local)

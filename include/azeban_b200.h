@@ -255,6 +255,65 @@ int az_debug_get_wait_limit(void);
  * (include/azeban/init/initializer.hpp:68-75). */
 az_status az_leray(int dim, long long N, int precision, void* u_hat, int batch, void* stream);
 
+/* ---- initial data (include/azeban/init/initializer.hpp:48-75) ------------
+ * The physical field is sampled on the device; az_fft_forward and az_leray
+ * then give the spectral state, as Initializer::initialize does. */
+
+enum {
+  AZ_INIT_TAYLOR_GREEN = 0,          /* src/azeban/init/taylor_green.cpp:29-46 (2-D), :146-184 (3-D),
+                                        with its perturbation modes (deltas) */
+  AZ_INIT_TAYLOR_GREEN_WORKLOAD = 1, /* (sin x cos y, -cos x sin y[, 0]) with cos z in 3-D (no counterpart) */
+  AZ_INIT_DOUBLE_SHEAR_LAYER = 2,    /* src/azeban/init/double_shear_layer.cpp:25-43, v = delta sin(2 pi x + phi) */
+  AZ_INIT_GAUSSIAN_NOISE = 3         /* independent standard normals (the random fields' white noise) */
+};
+
+typedef struct {
+  int kind;            /* AZ_INIT_* */
+  int dim;             /* 2 or 3 */
+  long long N;         /* grid points per axis */
+  int precision;       /* az_precision of the field */
+  int batch;           /* members; the field is [batch][dim][N]..[N] real */
+  double rho, delta;   /* double shear layer */
+  const double* deltas;  /* Taylor-Green perturbation amplitudes, host [batch][8 (2-D) | 24 (3-D)], or NULL */
+  const double* phases;  /* double-shear-layer phases, host [batch], or NULL: drawn from the random stream */
+  unsigned long long seed;  /* key of the random stream */
+  long long member0;        /* member b draws from stream (seed, member0 + b) */
+} az_init_desc;
+
+/* Samples the physical field of every member into u (device).  Random values
+ * (shear-layer phases when phases is NULL, Gaussian noise) come from the
+ * counter-based Philox4x32-10 stream (seed, member): value c of a stream is a
+ * function of (seed, member, c) alone.  The call waits for the stream only
+ * when deltas or phases are given (their copy to the device). */
+az_status az_init_physical(const az_init_desc* desc, void* u, void* stream);
+/* u_hat [batch][dim][N]([N])[N/2+1] *= |n|^exponent per mode (n the integer
+ * wavevector), 0 at n = 0: the amplitude envelope of a random field. */
+az_status az_init_envelope(int dim, long long N, int precision, void* u_hat, int batch, double exponent,
+                           void* stream);
+/* Scales every member of u_hat to kinetic energy 1/2 <|u|^2> = target
+ * (FP64 compensated sums on the device; nothing returns to the host). */
+az_status az_init_normalize_energy(int dim, long long N, int precision, void* u_hat, int batch, double target,
+                                   void* stream);
+/* Value index of stream (seed, member) as a uniform double in [0, 1): the
+ * draw the shear-layer phase takes (index 0), for the host. */
+az_status az_random_uniform(unsigned long long seed, unsigned long long member, unsigned long long index,
+                            double* out);
+/* The block function of the stream: Philox4x32-10 of counter[4] under
+ * key[2] (Salmon et al., SC 2011); stream (seed, member) block c has counter
+ * (c lo, c hi, member lo, member hi) and key (seed lo, seed hi). */
+az_status az_philox4x32_10(const unsigned* counter, const unsigned* key, unsigned* out);
+
+/* ---- measurement (no counterpart in the reference) ----------------------- */
+
+/* Times one radix-16 DFT stage of FP32 complex columns held in shared memory,
+ * over ctas CTAs of 128 columns, done with the transform passes' butterflies
+ * (method 0) or as a DFT-as-GEMM stage on the tensor pipe (method 1: the
+ * 32x32 real form of the DFT matrix times the columns, mma.sync m16n8k8 TF32
+ * with a three-term head/tail split for FP32 accuracy).  Writes the time per
+ * column and stage in ns and the largest error of one stage relative to the
+ * largest output (FP64 DFT reference). */
+az_status az_bench_radix16_stage(int method, int ctas, double* ns_per_column_stage, double* max_rel_err);
+
 /* ---- right-hand side without allocation (no counterpart in the reference) */
 
 /* Size of the one device array that az_euler_dudt_noalloc takes its scratch from. */

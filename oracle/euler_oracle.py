@@ -690,16 +690,34 @@ def _coords(N, d):
     return np.meshgrid(*([x] * d), indexing="ij")
 
 
-def taylor_green_reference(dim: int, N: int) -> np.ndarray:
-    """azeban's own Taylor-Green field without perturbation
-    (taylor_green.cpp:29-46 in 2-D, :146-166 in 3-D), physical space."""
+def taylor_green_reference(dim: int, N: int, deltas=None) -> np.ndarray:
+    """azeban's own Taylor-Green field (taylor_green.cpp:29-46 in 2-D,
+    :146-184 in 3-D), physical space, with its perturbation modes of
+    amplitudes deltas (8 in 2-D: d * 4 + {ss, sc, cs, cc} of (2x, 2y); 24 in
+    3-D: d * 8 + the eight sin/cos products of (2x, 2y, 2z)), or none."""
     if dim == 2:
         x, y = _coords(N, 2)
-        return np.stack([np.cos(x) * np.sin(y), -np.sin(x) * np.cos(y)])
+        u = [1.0 * np.cos(x) * np.sin(y), -1.0 * np.sin(x) * np.cos(y)]
+        if deltas is not None:
+            # left to right, as the reference multiplies: delta * f(2x) * g(2y)
+            fs = [(np.sin, np.sin), (np.sin, np.cos), (np.cos, np.sin), (np.cos, np.cos)]
+            for d in range(2):
+                for t, (f, g) in enumerate(fs):
+                    u[d] = u[d] + deltas[t + 4 * d] * f(2 * x) * g(2 * y)
+        return np.stack(u)
     x, y, z = _coords(N, 3)
-    return np.stack([np.cos(x) * np.sin(y) * np.sin(z),
-                     -np.sin(x) * np.cos(y) * np.sin(z),
-                     0.0 * x])
+    u = [1.0 * np.cos(x) * np.sin(y) * np.sin(z), -1.0 * np.sin(x) * np.cos(y) * np.sin(z),
+         0.0 * np.sin(x) * np.sin(y) * np.cos(z)]
+    if deltas is not None:
+        fx = [np.sin(2 * x), np.cos(2 * x)]
+        fy = [np.sin(2 * y), np.cos(2 * y)]
+        fz = [np.sin(2 * z), np.cos(2 * z)]
+        for d in range(3):
+            for t in range(8):
+                # delta * f(2x) * g(2y) * h(2z), left to right; t = 4 a + 2 b + c
+                a, b, c = t >> 2, (t >> 1) & 1, t & 1
+                u[d] = u[d] + deltas[t + 8 * d] * fx[a] * fy[b] * fz[c]
+    return np.stack(u)
 
 
 def taylor_green_workload(dim: int, N: int) -> np.ndarray:

@@ -59,3 +59,21 @@ def test_host_side_config_mirrors_reference():
         az.make_viscosity({"type": "Smooth Cutoff"}, g)
     with pytest.raises(ValueError):
         az.make_grid({"N_phys": 8, "N_fourier": 5}, 2)
+
+
+def test_philox_known_answers():
+    """The random stream's block function, Philox4x32-10, against the
+    known-answer vectors its authors publish with the algorithm (counter,
+    key -> output); a host call, no GPU."""
+    import ctypes as ct
+    from azeban_b200 import _lib
+    kat = [
+        ((0, 0, 0, 0), (0, 0), (0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8)),
+        ((0xFFFFFFFF,) * 4, (0xFFFFFFFF,) * 2, (0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD)),
+        ((0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344), (0xA4093822, 0x299F31D0),
+         (0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1)),
+    ]
+    for ctr, key, want in kat:
+        out = (ct.c_uint * 4)()
+        _lib.check(_lib.lib.az_philox4x32_10((ct.c_uint * 4)(*ctr), (ct.c_uint * 2)(*key), out))
+        assert tuple(out) == want
