@@ -293,10 +293,11 @@ def run_ours(args, rank, world, local):
     nl = (ct.c_longlong * 5)()
     _lib.check(_lib.lib.az_profile_read(ms, by, nl, 5))
     pass_names = ["inv_x_pad", "inv_y_pad", "z_product", "fwd_y_trunc", "fwd_x_epilogue"]
-    # The product pass runs k_zpass when bit 1 of its tuned variant is set.
+    # The product pass kernel: k_zfused (bit 2 of its tuned variant), k_zpass (bit 1) or k_rows_product.
     zv = ct.c_int()
     _lib.check(_lib.lib.az_tune_get(1, g.N_phys_pad, 1, ct.byref(zv)))
-    kernel_keys = ["k_cols_pad_inv_x", "k_cols_pad_inv_y", "k_zpass" if zv.value & 2 else "k_rows_product",
+    product_kernel = "k_zfused" if zv.value & 4 else "k_zpass" if zv.value & 2 else "k_rows_product"
+    kernel_keys = ["k_cols_pad_inv_x", "k_cols_pad_inv_y", product_kernel,
                    "k_cols_trunc_fwd", "k_fwd_epilogue"]
     peak, peak_kind = measured_peak_hbm()
     passes = {}
