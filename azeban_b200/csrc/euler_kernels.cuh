@@ -550,12 +550,16 @@ __global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NCM * Plan<L, V>::TPL,
   C* out = reinterpret_cast<C*>(a.out) + member * a.u_mem;
   const StateLayout lu = a.lu, lu0 = a.lu0, lout = a.lout;  // offsets < 2^31, checked by the launcher
   const T inv_k0sq = T(1.0 / (a.visc.k0 * a.visc.k0));
-  // The stage combination as uniform coefficients instead of per-element
-  // branches: t = u + dt d (d itself for MODE_DUDT), r = ct t + cw u0.
+  // The stage combination as a uniform coefficient instead of per-element
+  // branches: t = u + dt d (d itself for MODE_DUDT), r = ct t + (1 - ct) u0,
+  // evaluated as u0 + ct (t - u0) (u0 = 0 and ct = 1 for MODE_DUDT and
+  // MODE_RK1).  The weights then sum to exactly one in either precision: with
+  // the FP32 weights 2/3 and 1/3 the sum is 1 + 3e-8, which scales the state
+  // by that factor at every step.  t - u0 is exact while t and u0 lie within a
+  // factor of two (Sterbenz), so the form rounds once, in the fma.
   const bool use_u = a.mode != MODE_DUDT;
   const T dd = use_u ? dt : T(1);
   const T ct = a.mode == MODE_RK2 ? T(0.25) : a.mode == MODE_RK3 ? T(2.0 / 3.0) : T(1);
-  const T cw = a.mode == MODE_RK2 ? T(0.75) : a.mode == MODE_RK3 ? T(1.0 / 3.0) : T(0);
   // NT is a multiple of NCM, so a thread keeps one mode column pl (and its
   // second and third wavenumbers) and walks the retained rows i.
   const int pl = tid % NCM;
@@ -645,7 +649,7 @@ __global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NCM * Plan<L, V>::TPL,
       const C d = zero ? cmk<C>(T(0), T(0)) : cmk<C>(-Lh[c].x + nu * uc.x, -Lh[c].y + nu * uc.y);
       const C t = use_u ? cmk<C>(uc.x + dd * d.x, uc.y + dd * d.y) : d;
       const C w = wc_[c];
-      out[c * lout.comp + oo] = cmk<C>(ct * t.x + cw * w.x, ct * t.y + cw * w.y);
+      out[c * lout.comp + oo] = cmk<C>(fma(ct, t.x - w.x, w.x), fma(ct, t.y - w.y, w.y));
     }
   };
 #pragma unroll

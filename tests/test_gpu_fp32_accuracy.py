@@ -5,9 +5,9 @@ one-off rounding of the initial state would make it (the "floor" the bench
 reports).  This test shows the excess is what any FP32 evaluation of the same
 right-hand sides produces, not a defect of this library's kernels: the
 oracle's single-precision evaluation (pocketfft float32 transforms, float32
-products, dudt_slabs(single=True)) stepped with SSP-RK3 and its state kept in
-complex64 after every stage, as the FP32-bulk form keeps it, lands at the same
-error.  Taylor-Green 3-D N = 32 (the bench's field) to azeban t = 1/(2 pi)
+products, FP64 per-mode arithmetic: dudt_slabs(single=True)) stepped with
+SSP-RK3 and its state kept in complex64 after every stage, as the FP32-bulk
+form keeps it, lands within a factor of two of it.  Taylor-Green 3-D N = 32 (the bench's field) to azeban t = 1/(2 pi)
 and t = 1 (t = 1 and 2 pi on [0, 2 pi)^3).
 
 Tolerance: the library's FP32 error at most twice the single-precision
