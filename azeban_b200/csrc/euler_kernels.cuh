@@ -68,7 +68,11 @@ struct ColArgs {
 
 // Batched column transforms along a strided axis.  grid = (ntile * nouter,
 // ncomp, nmembers); block = NC * L/E threads.
-template <typename T, int L, int NC, int S, int MODE, int V>
+// STD: the unpadded length is 2L/3 (the 3/2 rule, a.n_short == 2L/3), known at
+// compile time, so the padding and truncation maps fold: rows whose fate does
+// not depend on the thread's row offset are kept, zeroed or dropped without a
+// test.
+template <typename T, int L, int NC, int S, int MODE, int V, bool STD = false>
 __global__ void __launch_bounds__(NC * Plan<L, V>::TPL) k_cols(ColArgs a) {
   using C = cvec<T>;
   using P = Plan<L, V>;
@@ -104,7 +108,7 @@ __global__ void __launch_bounds__(NC * Plan<L, V>::TPL) k_cols(ColArgs a) {
   const C* in = reinterpret_cast<const C*>(a.in) + member * a.in_mem + outer * a.in_outer + pin;
   C* out = reinterpret_cast<C*>(a.out) + member * a.out_mem + comp * a.out_comp +
            outer * a.out_outer + p;
-  const int n = a.n_short;
+  const int n = STD ? 2 * L / 3 : a.n_short;
   // Row offsets fit 32 bits (the launcher checks L * stride < 2^31).
   const int in_row = int(a.in_row);
   const int out_row = int(a.out_row);
@@ -495,7 +499,9 @@ template <typename T, int L, int NCM, int DIM, int V> struct EpiMinBlocks {
   static constexpr int value = (sizeof(T) == 4 && V == 0) ? 2 : 1;
 };
 
-template <typename T, int L, int NCM, int DIM, int V>
+// STD: N == 2L/3 (the 3/2 rule), known at compile time, so the retained-row
+// map and the per-mode row loops fold.
+template <typename T, int L, int NCM, int DIM, int V, bool STD = false>
 __global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NCM * Plan<L, V>::TPL,
                                   EpiMinBlocks<T, L, NCM, DIM, V>::value)
     k_fwd_epilogue(EpiArgs a) {
@@ -513,7 +519,7 @@ __global__ void __launch_bounds__((DIM * (DIM + 1) / 2) * NCM * Plan<L, V>::TPL,
   if (a.ctrl != nullptr && a.ctrl[member].skip) return;
   const int tid = threadIdx.x;
   const int tile = blockIdx.x;
-  const int N = a.N;
+  const int N = STD ? 2 * L / 3 : a.N;
   {
     // column col = (mode pl, component c) with c fastest: one contiguous run
     const int col = tid % NC;

@@ -97,15 +97,25 @@ template <typename T, int L, int V> struct LaunchV {
   using TS = Tiles<T, L, V>;
   static constexpr int TPL = Plan<L, V>::TPL;
 
-  template <int S, int MODE>
-  static cudaError_t col_kernel(const ColArgs& a, dim3 g, cudaStream_t st) {
+  template <int S, int MODE, bool STD>
+  static cudaError_t col_kernel_(const ColArgs& a, dim3 g, cudaStream_t st) {
     constexpr int NC = TS::NC;
     const size_t smem = size_t(L + L * NC) * sizeof(C);
-    auto k = k_cols<T, L, NC, S, MODE, V>;
+    auto k = k_cols<T, L, NC, S, MODE, V, STD>;
     static const cudaError_t attr = set_smem(k, smem);
     if (attr != cudaSuccess) return attr;
     k<<<g, NC * TPL, smem, st>>>(a);
     return cudaGetLastError();
+  }
+
+  // The padding and truncating passes of the 3/2 rule (n == 2L/3) take the
+  // form with the maps folded at compile time.
+  template <int S, int MODE>
+  static cudaError_t col_kernel(const ColArgs& a, dim3 g, cudaStream_t st) {
+    if constexpr (MODE != COL_PLAIN && L % 3 == 0) {
+      if (3LL * a.n_short == 2LL * L) return col_kernel_<S, MODE, true>(a, g, st);
+    }
+    return col_kernel_<S, MODE, false>(a, g, st);
   }
 
   // The column kernels index rows with 32-bit offsets.
@@ -204,12 +214,21 @@ template <typename T, int L, int V> struct LaunchV {
     return cudaErrorInvalidValue;
   }
 
-  // k_zfused with forward plan V (this struct's) and inverse plan VI.
+  // k_zfused with forward plan V (this struct's) and inverse plan VI; the
+  // form with nh folded at compile time for the 3/2 rule (nh == L/3 + 1).
   template <int DIM, int VI>
   static cudaError_t zfused(const ZArgs& a0, cudaStream_t st) {
+    if constexpr (L % 3 == 0) {
+      if (a0.nh == L / 3 + 1) return zfused_<DIM, VI, true>(a0, st);
+    }
+    return zfused_<DIM, VI, false>(a0, st);
+  }
+
+  template <int DIM, int VI, bool STD>
+  static cudaError_t zfused_(const ZArgs& a0, cudaStream_t st) {
     constexpr int NLP = ZFTile<T, L, DIM, V>::NLP;
     using Z = ZFShape<T, L, NLP, DIM, V, VI>;
-    auto k = k_zfused<T, L, NLP, DIM, V, VI>;
+    auto k = k_zfused<T, L, NLP, DIM, V, VI, STD>;
     if (a0.in_line < a0.nh * DIM || a0.out_line < a0.nh * Z::NB) return cudaErrorInvalidValue;
     // Each pair's bulk copy needs 16-byte aligned source, destination and size.
     const long long pair_bytes = 2LL * a0.in_line * Z::CB;
@@ -242,15 +261,23 @@ template <typename T, int L, int V> struct LaunchV {
     return cudaErrorInvalidValue;
   }
 
-  template <int DIM, int NCM>
-  static cudaError_t epi_kernel(const EpiArgs& a, dim3 g, cudaStream_t st) {
+  template <int DIM, int NCM, bool STD>
+  static cudaError_t epi_kernel_(const EpiArgs& a, dim3 g, cudaStream_t st) {
     constexpr int NB = DIM * (DIM + 1) / 2;
     const size_t smem = size_t(L + L * NB * NCM) * sizeof(C);
-    auto k = k_fwd_epilogue<T, L, NCM, DIM, V>;
+    auto k = k_fwd_epilogue<T, L, NCM, DIM, V, STD>;
     static const cudaError_t attr = set_smem(k, smem);
     if (attr != cudaSuccess) return attr;
     k<<<g, NB * NCM * TPL, smem, st>>>(a);
     return cudaGetLastError();
+  }
+
+  template <int DIM, int NCM>
+  static cudaError_t epi_kernel(const EpiArgs& a, dim3 g, cudaStream_t st) {
+    if constexpr (L % 3 == 0) {
+      if (3LL * a.N == 2LL * L) return epi_kernel_<DIM, NCM, true>(a, g, st);
+    }
+    return epi_kernel_<DIM, NCM, false>(a, g, st);
   }
 
   static cudaError_t epi(int dim, const EpiArgs& a, dim3 g, cudaStream_t st) {

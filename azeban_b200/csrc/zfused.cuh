@@ -73,7 +73,10 @@ template <typename T, int L, int NLP, int DIM, int VF, int VI> struct ZFShape {
   }
 };
 
-template <typename T, int L, int NLP, int DIM, int VF, int VI>
+// STD: nh == L/3 + 1 (the 3/2 rule), known at compile time, so the Hermitian
+// read pattern of the inverse transform's first stage and the separation loop
+// fold.
+template <typename T, int L, int NLP, int DIM, int VF, int VI, bool STD = false>
 __global__ void __launch_bounds__(ZFShape<T, L, NLP, DIM, VF, VI>::NT, ZFShape<T, L, NLP, DIM, VF, VI>::MINB)
     k_zfused(ZArgs a) {
   using C = cvec<T>;
@@ -92,7 +95,7 @@ __global__ void __launch_bounds__(ZFShape<T, L, NLP, DIM, VF, VI>::NT, ZFShape<T
   Ctrl* ctrl = a.ctrl + member;
   if (ctrl->skip) return;
   const int tid = threadIdx.x;
-  const int nh = a.nh;
+  const int nh = STD ? L / 3 + 1 : a.nh;
   const int in_line = a.in_line;
   const int out_line = a.out_line;
   const int pstride = a.pstride;
