@@ -369,34 +369,49 @@ def run_ours(args, rank, world, local):
     # ---- end to end through the public API with host buffers ---------------
     # A step is the host->device copy of the batch's state from pinned memory,
     # one SSP-RK3 step of the batch (Simulation.steps, no host sync) and the
-    # device->host copy of the new state.  Batched Simulations on their own
-    # streams take steps in turn: one step's chain (copy in, transforms, copy
-    # out) is about 2.6 steps of transform time at the host link's duplex
-    # rate, so three in flight keep the transforms and both copy directions
-    # busy (measured: 2 -> 143, 3 -> 188, 4 -> 164 member-steps/s; one
-    # Simulation per member on its own stream: 164-175).
+    # device->host copy of the new state.  NBUF batched Simulations take steps
+    # in turn: their steps run in order on one compute stream (no two steps
+    # share the SMs), while a copy-in stream fills the next batch's state and
+    # a copy-out stream drains the previous one, chained by events.  The host
+    # link bounds it: 0.81 GB each way per step of 4 members take 16.2 ms
+    # when both directions run at once and 18.1-18.8 ms per step pipelined
+    # without any transform (measured for 2 to 6 buffers), against 17.4 ms
+    # of transforms; with both, 19.9-20.4 ms per step.  Three buffers: a
+    # batch's copy-in waits for its own previous copy-out.
     e2e = None
     if not args.no_e2e:
         NBUF = 3
         host_in = batch_u.cpu().pin_memory()
         host_out = [torch.empty_like(host_in).pin_memory() for _ in range(NBUF)]
-        streams = [torch.cuda.Stream() for _ in range(NBUF)]
+        s_in, s_comp, s_out = torch.cuda.Stream(), torch.cuda.Stream(), torch.cuda.Stream()
         esims = [az.Simulation(g, C_CFL, az.SSP_RK3(az.IncompressibleEuler(g, visc, "f32", B)), batch_u)
                  for _ in range(NBUF)]
+        out_done = [None] * NBUF
         torch.cuda.synchronize()
 
         def e2e_steps(n, start_evt=None):
             if start_evt is not None:
-                for sb in streams:
+                for sb in (s_in, s_comp, s_out):
                     sb.wait_event(start_evt)
             for k in range(n):
                 j = k % NBUF
-                with torch.cuda.stream(streams[j]):
-                    u_dev = esims[j].u()
+                u_dev = esims[j].u()
+                if out_done[j] is not None:
+                    s_in.wait_event(out_done[j])
+                with torch.cuda.stream(s_in):
                     u_dev.copy_(host_in, non_blocking=True)
-                    esims[j].steps(1, stream=streams[j])
+                in_done = torch.cuda.Event()
+                in_done.record(s_in)
+                s_comp.wait_event(in_done)
+                esims[j].steps(1, stream=s_comp)
+                comp_done = torch.cuda.Event()
+                comp_done.record(s_comp)
+                s_out.wait_event(comp_done)
+                with torch.cuda.stream(s_out):
                     host_out[j].copy_(u_dev, non_blocking=True)
-            for sb in streams:
+                out_done[j] = torch.cuda.Event()
+                out_done[j].record(s_out)
+            for sb in (s_in, s_comp, s_out):
                 ev = torch.cuda.Event()
                 ev.record(sb)
                 stream.wait_event(ev)
@@ -413,7 +428,8 @@ def run_ours(args, rank, world, local):
         nbytes = host_in.numel() * host_in.element_size()
         e2e = {"value": world * B * K / (te / 1e3), "unit": UNIT, "h2d_bytes_per_step": nbytes,
                "d2h_bytes_per_step": nbytes,
-               "form": f"{NBUF} batched Simulations ({B} members each) on their own streams, taking alternate steps"}
+               "form": f"{NBUF} batched Simulations ({B} members each) taking steps in turn on one compute stream, "
+                       "copies in and out on two copy streams"}
         del esims
 
     # ---- CPU baseline (rank 0, N = 1) ---------------------------------------
