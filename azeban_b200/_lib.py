@@ -38,7 +38,7 @@ EXPORTS = [
     "az_group_steps", "az_group_steps_active", "az_group_set_end", "az_group_simulate_until",
     "az_debug_set_wait_limit", "az_debug_get_wait_limit", "az_euler_noalloc_status",
     "az_init_physical", "az_init_envelope", "az_init_normalize_energy", "az_random_uniform",
-    "az_philox4x32_10", "az_bench_radix16_stage",
+    "az_philox4x32_10", "az_bench_radix16_stage", "az_bench_exchange384",
 ]
 
 
@@ -131,6 +131,7 @@ def _load():
         "az_random_uniform": (I, [ct.c_ulonglong, ct.c_ulonglong, ct.c_ulonglong, ct.POINTER(D)]),
         "az_philox4x32_10": (I, [ct.POINTER(ct.c_uint), ct.POINTER(ct.c_uint), ct.POINTER(ct.c_uint)]),
         "az_bench_radix16_stage": (I, [I, I, ct.POINTER(D), ct.POINTER(D)]),
+        "az_bench_exchange384": (I, [I, I, ct.POINTER(D), ct.POINTER(D)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

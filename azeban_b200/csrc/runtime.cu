@@ -105,6 +105,9 @@ static int g_wait_polls = kWaitPolls;
 static std::mutex g_tw_mutex;
 static std::map<std::tuple<int, int, int>, void*> g_tw;
 
+static az_status twiddles(int precision, int L, const void** out);
+az_status device_twiddles(int precision, int L, const void** out) { return twiddles(precision, L, out); }
+
 static az_status twiddles(int precision, int L, const void** out) {
   int dev = 0;
   AZB_CUDA(cudaGetDevice(&dev));

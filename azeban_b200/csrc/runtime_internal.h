@@ -63,6 +63,9 @@ az_status set_error(az_status st, const char* msg);
 // AZ_OK for a zero Ctrl::err word, else the status (and message) it encodes:
 // bit 1 AZ_ERR_TIMEOUT, bit 0 AZ_ERR_NONFINITE.
 az_status ctrl_status(int err);
+// The device twiddle table W_L^m (m in [0, L)) of the current device, built
+// once per (device, precision, L) and kept until exit.
+az_status device_twiddles(int precision, int L, const void** out);
 // Compiled kernels of one (precision, transform length), or nullptr.
 const KernelSet* find_kernel_set(int precision, int L);
 // Plan variant (0 std, 1 wide) the tuning table holds for a pass kind

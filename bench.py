@@ -56,7 +56,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workload", default="tg3d256",
                     choices=["tg3d256", "tg2d64", "tg3d-accuracy", "dsl-ensemble", "fbm512", "serving",
-                             "dft-gemm-stage"],
+                             "dft-gemm-stage", "exchange"],
                     help="tg3d256 is the headline; the others are the remaining workloads, one JSON line each")
     ap.add_argument("--duration", type=float, default=60.0, help="serving: seconds of Poisson arrivals")
     ap.add_argument("--rate", type=float, default=200.0, help="serving: arrivals per second")
@@ -753,6 +753,27 @@ def run_dft_gemm_stage(args):
                                   f"{8 * sms} CTAs of 128 columns", "results": res}), flush=True)
 
 
+def run_exchange(args):
+    """The 384-point FP32 transform of the wide plan (radix 16, exchange,
+    radix 24) on every SM, with the exchange through shared memory (the
+    transform passes' way) or as a lane transpose with warp shuffles: time per
+    column transform and the error of one transform."""
+    import ctypes as ct
+
+    import torch
+
+    from azeban_b200 import _lib
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    res = {}
+    for name, method in (("shared_memory", 0), ("warp_shuffle", 1), ("warp_shuffle_uncapped", 2)):
+        ns, err = ct.c_double(), ct.c_double()
+        _lib.check(_lib.lib.az_bench_exchange384(method, 16 * sms, ct.byref(ns), ct.byref(err)))
+        res[name] = {"ns_per_column": ns.value, "max_rel_err": err.value}
+    res["shuffle_over_shared_time"] = res["warp_shuffle"]["ns_per_column"] / res["shared_memory"]["ns_per_column"]
+    print(json.dumps({"workload": "384-point FP32 transform (16 x 24), exchange through shared memory vs warp "
+                                  f"shuffles, {16 * sms} CTAs of 32 columns", "results": res}), flush=True)
+
+
 def launch_ranks(args):
     """--gpus N without a launcher: re-run this command under
     torch.distributed.run with N ranks on this node (one per GPU, rendezvous
@@ -797,7 +818,8 @@ def main():
         run_reference(args, rank, world)
         return
     extra = {"tg2d64": run_tg2d64, "tg3d-accuracy": run_tg3d_accuracy, "dsl-ensemble": run_dsl_ensemble,
-             "fbm512": run_fbm512, "serving": run_serving, "dft-gemm-stage": run_dft_gemm_stage}
+             "fbm512": run_fbm512, "serving": run_serving, "dft-gemm-stage": run_dft_gemm_stage,
+             "exchange": run_exchange}
     if args.workload in extra:
         import torch
         torch.cuda.set_device(local)

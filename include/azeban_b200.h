@@ -314,6 +314,16 @@ az_status az_philox4x32_10(const unsigned* counter, const unsigned* key, unsigne
  * largest output (FP64 DFT reference). */
 az_status az_bench_radix16_stage(int method, int ctas, double* ns_per_column_stage, double* max_rel_err);
 
+/* Times the 384-point FP32 transform of the wide plan (radix 16, one
+ * exchange, radix 24; 8 threads per column) over ctas CTAs of 32 columns held
+ * in registers, with the exchange between the stages done through shared
+ * memory as the transform passes do (method 0) or as a lane transpose with
+ * warp shuffles among each column's 8 consecutive lanes (method 1: two CTAs
+ * per SM as method 0; method 2: registers uncapped, one CTA per SM).  Writes
+ * the time per column transform in ns and the largest error of one transform
+ * relative to the largest output (FP64 DFT reference). */
+az_status az_bench_exchange384(int method, int ctas, double* ns_per_column, double* max_rel_err);
+
 /* ---- right-hand side without allocation (no counterpart in the reference) */
 
 /* Size of the one device array that az_euler_dudt_noalloc takes its scratch from. */
