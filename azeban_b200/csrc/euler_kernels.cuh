@@ -494,9 +494,10 @@ template <typename T> __device__ __forceinline__ T visc_from_k2(const Visc& v, T
 //   MODE_RK2:  out = 3/4 u0 + 1/4 (u + dt dudt)       (ssp_rk3.hpp:57-58)
 //   MODE_RK3:  out = 2/3 (u + dt dudt) + 1/3 u0       (ssp_rk3.hpp:60-61)
 // grid = (ntile, nmembers); block = NB * NCM * L/E.
-// FP32 std plans: two resident CTAs per SM.
+// FP32 std plans of up to 384 threads: two resident CTAs per SM.
 template <typename T, int L, int NCM, int DIM, int V> struct EpiMinBlocks {
-  static constexpr int value = (sizeof(T) == 4 && V == 0) ? 2 : 1;
+  static constexpr int value =
+      (sizeof(T) == 4 && V == 0 && (DIM * (DIM + 1) / 2) * NCM * Plan<L, V>::TPL <= 384) ? 2 : 1;
 };
 
 // STD: N == 2L/3 (the 3/2 rule), known at compile time, so the retained-row

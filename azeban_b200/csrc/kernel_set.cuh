@@ -11,12 +11,21 @@
 
 namespace azb {
 
-enum ColKind : int { COLK_PAD_INV = 0, COLK_PLAIN_INV = 1, COLK_TRUNC_FWD = 2, COLK_PLAIN_FWD = 3 };
+// COLK_PAD_INV_WIDE: the padding inverse pass that reads the state (the first
+// pass of a 3-D right-hand side), on tiles of TileShape::ncx columns.
+enum ColKind : int {
+  COLK_PAD_INV = 0,
+  COLK_PLAIN_INV = 1,
+  COLK_TRUNC_FWD = 2,
+  COLK_PLAIN_FWD = 3,
+  COLK_PAD_INV_WIDE = 4
+};
 
 // Tile shapes of one (precision, L).  Threads per CTA and shared memory
 // follow from them; they are the knobs a tuner turns.
 struct TileShape {
   int nc;     // columns per CTA, column passes
+  int ncx;    // columns per CTA, the first (state-reading) pass of a 3-D right-hand side
   int nlp2;   // line pairs per CTA, 2-D product pass
   int nlp3;   // line pairs per CTA, 3-D product pass
   int ncm2;   // modes per CTA, 2-D epilogue pass
@@ -50,9 +59,17 @@ constexpr int kclamp(int x, int lo, int hi) { return x < lo ? lo : (x > hi ? hi 
 template <typename T, int L, int V> struct Tiles {
   static constexpr int CB = int(sizeof(cvec<T>));
   static constexpr int NC = kclamp(kpow2floor(49152 / (L * CB)), 2, 32);
+  // The first pass reads the state in runs of NCX elements per row, rows a
+  // plane apart: at least 128 bytes per run where the shared-memory budget
+  // of NC allows fewer (measured at L = 768 in FP32: 16 columns 1.48 ms
+  // against 8 columns 1.96 ms at 512^3; the other column passes keep NC, for
+  // which 16 columns were slower).
+  static constexpr int NCX = (CB == 8 && NC * CB < 128 && L <= 768) ? 128 / CB : NC;
   static constexpr int NLP3 = kclamp(kpow2floor(81920 / (L * 6 * CB)), 1, 16);
   static constexpr int NLP2 = kclamp(kpow2floor(81920 / (L * 3 * CB)), 1, 16);
-  static constexpr int NCM3 = kclamp(kpow2floor(81920 / (L * 6 * CB)), 1, 16);
+  // FP32 at L = 768: twice the budget, 4 modes per CTA (one CTA per SM;
+  // measured 2.95 ms against 3.67 ms with 2 modes at 512^3).
+  static constexpr int NCM3 = kclamp(kpow2floor(((CB == 8 && L == 768) ? 163840 : 81920) / (L * 6 * CB)), 1, 16);
   static constexpr int NCM2 = kclamp(kpow2floor(81920 / (L * 3 * CB)), 1, 16);
   static constexpr int NLPR = kclamp(kpow2floor(49152 / (L * CB)), 1, 64);
 };
@@ -97,9 +114,8 @@ template <typename T, int L, int V> struct LaunchV {
   using TS = Tiles<T, L, V>;
   static constexpr int TPL = Plan<L, V>::TPL;
 
-  template <int S, int MODE, bool STD>
+  template <int S, int MODE, bool STD, int NC>
   static cudaError_t col_kernel_(const ColArgs& a, dim3 g, cudaStream_t st) {
-    constexpr int NC = TS::NC;
     const size_t smem = size_t(L + L * NC) * sizeof(C);
     auto k = k_cols<T, L, NC, S, MODE, V, STD>;
     static const cudaError_t attr = set_smem(k, smem);
@@ -110,12 +126,12 @@ template <typename T, int L, int V> struct LaunchV {
 
   // The padding and truncating passes of the 3/2 rule (n == 2L/3) take the
   // form with the maps folded at compile time.
-  template <int S, int MODE>
+  template <int S, int MODE, int NC = TS::NC>
   static cudaError_t col_kernel(const ColArgs& a, dim3 g, cudaStream_t st) {
     if constexpr (MODE != COL_PLAIN && L % 3 == 0) {
-      if (3LL * a.n_short == 2LL * L) return col_kernel_<S, MODE, true>(a, g, st);
+      if (3LL * a.n_short == 2LL * L) return col_kernel_<S, MODE, true, NC>(a, g, st);
     }
-    return col_kernel_<S, MODE, false>(a, g, st);
+    return col_kernel_<S, MODE, false, NC>(a, g, st);
   }
 
   // The column kernels index rows with 32-bit offsets.
@@ -156,6 +172,7 @@ template <typename T, int L, int V> struct LaunchV {
       case COLK_PLAIN_INV: return col_kernel<+1, COL_PLAIN>(a, g, st);
       case COLK_TRUNC_FWD: return col_kernel<-1, COL_TRUNC>(a, g, st);
       case COLK_PLAIN_FWD: return col_kernel<-1, COL_PLAIN>(a, g, st);
+      case COLK_PAD_INV_WIDE: return col_kernel<+1, COL_PAD, TS::NCX>(a, g, st);
       default: return cudaErrorInvalidValue;
     }
   }
@@ -312,7 +329,7 @@ template <typename T, int L, int V> struct LaunchV {
     return cudaGetLastError();
   }
 
-  static TileShape tiles() { return {TS::NC, TS::NLP2, TS::NLP3, TS::NCM2, TS::NCM3, TS::NLPR}; }
+  static TileShape tiles() { return {TS::NC, TS::NCX, TS::NLP2, TS::NLP3, TS::NCM2, TS::NCM3, TS::NLPR}; }
 };
 
 template <typename T, int L> struct Launch {

@@ -409,12 +409,15 @@ static az_status rhs(az_euler e, const void* u, bool u_inner, const void* u0, bo
   if (e->dim == 3) {
     // pass 1: inverse along x with padding, state [3][N][N][Nh] -> A1 [M][N][r3]
     // (column p: group y = p / r3, entry q = 3 z + component, q < 3 Nh)
+    // (the single-tile kernel runs it on the wider tiles of the first pass)
+    const bool wide = !(e->v_cols & 2);
+    const int nc1 = wide ? ks->tiles[e->v_cols & 1].ncx : nc;
     ColArgs a1{};
     a1.in = u;
     a1.out = e->buf[0];
     a1.tw = e->tw;
     a1.ninner = N * e->ra1;
-    a1.ntile = int(cdiv(a1.ninner, nc));
+    a1.ntile = int(cdiv(a1.ninner, nc1));
     a1.n_short = int(N);
     a1.in_row = u_inner ? 3 * N * Nh : N * Nh;
     a1.out_row = N * e->ra1;
@@ -433,7 +436,7 @@ static az_status rhs(az_euler e, const void* u, bool u_inner, const void* u0, bo
     a1.clear_max = 1;
     {
       ProfScope ps(P_INV_X, double(B) * 3 * (N * N * Nh + M * N * Nh) * e->csize, st, e->prof);
-      ce = ks->cols(e->v_cols, COLK_PAD_INV, a1, unsigned(a1.ntile), 1, B, st);
+      ce = ks->cols(e->v_cols, wide ? COLK_PAD_INV_WIDE : COLK_PAD_INV, a1, unsigned(a1.ntile), 1, B, st);
     }
     if (ce != cudaSuccess) return cuda_fail(ce, "rhs pass 1");
     // pass 2: inverse along y with padding, A1 -> A2 [M][M][r3]
