@@ -141,38 +141,41 @@ az_status az_bench_exchange384(int method, int ctas, double* ns_per_column, doub
   cudaError_t ce = cudaFuncSetAttribute(method == 0 ? k_exchange384<0, 2> : method == 1 ? k_exchange384<1, 2>
                                                                                        : k_exchange384<1, 1>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-  cudaEvent_t e0, e1;
-  cudaEventCreate(&e0);
-  cudaEventCreate(&e1);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (ce == cudaSuccess) ce = cudaEventCreate(&e0);
+  if (ce == cudaSuccess) ce = cudaEventCreate(&e1);
   auto launch = [&](int reps) {
     const float2* t = static_cast<const float2*>(tw);
     if (method == 0) k_exchange384<0, 2><<<ctas, kXbThreads, smem>>>(din, dout, t, reps);
     else if (method == 1) k_exchange384<1, 2><<<ctas, kXbThreads, smem>>>(din, dout, t, reps);
     else k_exchange384<1, 1><<<ctas, kXbThreads, smem>>>(din, dout, t, reps);
   };
-  auto timed = [&](int reps) {
+  auto timed = [&](int reps, double* ms_out) {
     launch(reps);  // warm-up
     cudaEventRecord(e0);
     launch(reps);
     cudaEventRecord(e1);
-    cudaEventSynchronize(e1);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
     float ms = 0;
-    cudaEventElapsedTime(&ms, e0, e1);
-    return double(ms);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    *ms_out = double(ms);
+    return e;
   };
   if (ce == cudaSuccess) ce = cudaMemcpy(din, h.data(), n * sizeof(float2), cudaMemcpyHostToDevice);
   double t1 = 0, t2 = 0;
   const int r1 = 8, r2 = 40;
+  if (ce == cudaSuccess) ce = timed(r1, &t1);
+  if (ce == cudaSuccess) ce = timed(r2, &t2);
   if (ce == cudaSuccess) {
-    t1 = timed(r1);
-    t2 = timed(r2);
     launch(1);  // one transform, for the accuracy check
-    ce = cudaMemcpy(outh.data(), dout, n * sizeof(float2), cudaMemcpyDeviceToHost);
+    ce = cudaGetLastError();
   }
+  if (ce == cudaSuccess) ce = cudaMemcpy(outh.data(), dout, n * sizeof(float2), cudaMemcpyDeviceToHost);
   cudaFree(din);
   cudaFree(dout);
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
   if (ce != cudaSuccess) return set_error(AZ_ERR_CUDA, cudaGetErrorString(ce));
   *ns_per_column = (t2 - t1) * 1e6 / (double(r2 - r1) * ctas * kXbCols);
   // accuracy of one transform against an FP64 DFT on a few columns

@@ -163,36 +163,45 @@ az_status az_bench_radix16_stage(int method, int ctas, double* ns_per_column_sta
   for (auto& v : h) v = make_float2(dist(rng), dist(rng));
   float2* d = nullptr;
   if (cudaMalloc(&d, n * sizeof(float2)) != cudaSuccess) return set_error(AZ_ERR_NOMEM, "az_bench_radix16_stage");
-  cudaEvent_t e0, e1;
-  cudaEventCreate(&e0);
-  cudaEventCreate(&e1);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaError_t ce = cudaEventCreate(&e0);
+  if (ce == cudaSuccess) ce = cudaEventCreate(&e1);
   auto launch = [&](int reps) {
     if (method == 0) k_stage_butterfly<<<ctas, kSbThreads>>>(d, reps);
     else k_stage_gemm<<<ctas, kSbThreads>>>(d, reps);
   };
-  auto timed = [&](int reps) {
-    cudaMemcpy(d, h.data(), n * sizeof(float2), cudaMemcpyHostToDevice);
+  auto timed = [&](int reps, double* ms_out) {
+    cudaError_t e = cudaMemcpy(d, h.data(), n * sizeof(float2), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return e;
     launch(reps);  // warm-up
-    cudaMemcpy(d, h.data(), n * sizeof(float2), cudaMemcpyHostToDevice);
+    e = cudaMemcpy(d, h.data(), n * sizeof(float2), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return e;
     cudaEventRecord(e0);
     launch(reps);
     cudaEventRecord(e1);
-    cudaEventSynchronize(e1);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
     float ms = 0;
-    cudaEventElapsedTime(&ms, e0, e1);
-    return double(ms);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    *ms_out = double(ms);
+    return e;
   };
   const int r1 = 16, r2 = 80;
-  const double t1 = timed(r1), t2 = timed(r2);
-  *ns_per_column_stage = (t2 - t1) * 1e6 / (double(r2 - r1) * ctas * kSbCols);
+  double t1 = 0, t2 = 0;
+  if (ce == cudaSuccess) ce = timed(r1, &t1);
+  if (ce == cudaSuccess) ce = timed(r2, &t2);
   // accuracy of one stage against an FP64 DFT
-  cudaMemcpy(d, h.data(), n * sizeof(float2), cudaMemcpyHostToDevice);
-  launch(1);
-  cudaError_t ce = cudaMemcpy(out.data(), d, n * sizeof(float2), cudaMemcpyDeviceToHost);
+  if (ce == cudaSuccess) ce = cudaMemcpy(d, h.data(), n * sizeof(float2), cudaMemcpyHostToDevice);
+  if (ce == cudaSuccess) {
+    launch(1);
+    ce = cudaGetLastError();
+  }
+  if (ce == cudaSuccess) ce = cudaMemcpy(out.data(), d, n * sizeof(float2), cudaMemcpyDeviceToHost);
   cudaFree(d);
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
   if (ce != cudaSuccess) return set_error(AZ_ERR_CUDA, cudaGetErrorString(ce));
+  *ns_per_column_stage = (t2 - t1) * 1e6 / (double(r2 - r1) * ctas * kSbCols);
   double err = 0, ref_max = 0;
   const int check = ctas < 8 ? ctas : 8;
   for (int b = 0; b < check; ++b)
