@@ -56,7 +56,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workload", default="tg3d256",
                     choices=["tg3d256", "tg2d64", "tg3d-accuracy", "dsl-ensemble", "fbm512", "serving",
-                             "dft-gemm-stage", "exchange"],
+                             "dft-gemm-stage", "exchange", "dsl-classes"],
                     help="tg3d256 is the headline; the others are the remaining workloads, one JSON line each")
     ap.add_argument("--duration", type=float, default=60.0, help="serving: seconds of Poisson arrivals")
     ap.add_argument("--rate", type=float, default=200.0, help="serving: arrivals per second")
@@ -579,6 +579,57 @@ def run_tg3d_accuracy(args):
     print(json.dumps({"workload": "TG-3D accuracy FP32 bulk vs FP64", "results": out}), flush=True)
 
 
+def run_dsl_classes(args):
+    """Each class of the DSL-2D ensemble alone (FP32 bulk, at its ensemble
+    batch size): 20 timed Simulation.steps(1) calls after 3 warm-up steps, and
+    the per-pass times from the library's per-pass CUDA events.  Model bytes
+    per member-step (fused axis-pass model, 2-D): 22 N Nh + 30 M Nh complex
+    elements."""
+    import ctypes as ct
+
+    import numpy as np
+    import torch
+
+    import azeban_b200 as az
+    from azeban_b200 import _lib
+    from azeban_b200 import init as azinit
+    rng = np.random.default_rng(2024)
+    rows = []
+    for N, B in [(128, 256), (256, 192), (512, 64)]:
+        g = az.Grid(2, N)
+        M, Nh = g.N_phys_pad, N // 2 + 1
+        eq = az.IncompressibleEuler(g, az.make_viscosity(VISC_CFG, g), "f32", batch=B)
+        u0 = azinit.double_shear_layer(N, math.pi / 15, 0.05, rng.uniform(0, 2 * math.pi, B), "f32")
+        sim = az.Simulation(g, C_CFL, az.SSP_RK3(eq), u0)
+        sim.steps(3)
+        torch.cuda.synchronize()
+        e0, e1 = _ev(), _ev()
+        e0.record()
+        for _ in range(20):
+            sim.steps(1)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 20
+        _lib.check(_lib.lib.az_profile_enable(1))
+        sim.steps(5)
+        torch.cuda.synchronize()
+        _lib.check(_lib.lib.az_profile_enable(0))
+        t = (ct.c_double * 5)()
+        by = (ct.c_double * 5)()
+        nl = (ct.c_longlong * 5)()
+        _lib.check(_lib.lib.az_profile_read(t, by, nl, 5))
+        model = (22 * N * Nh + 30 * M * Nh) * 8.0
+        passes = {}
+        for i, name in ((0, "inv_x_pad"), (2, "product"), (4, "epilogue")):
+            if nl[i]:
+                passes[name] = {"us": 1e3 * t[i] / nl[i], "gbs": by[i] / nl[i] / (t[i] / nl[i] * 1e6)}
+        rows.append({"N": N, "batch": B, "ms_per_step": ms, "member_steps_per_s": B / (ms / 1e3),
+                     "model_gbs": B * model / (ms / 1e3) / 1e9, "passes": passes})
+        del sim, eq
+    print(json.dumps({"workload": "DSL-2D classes each alone, FP32 bulk, ensemble batch sizes", "results": rows}),
+          flush=True)
+
+
 def run_dsl_ensemble(args):
     """2-D double-shear-layer ensemble, 512 members of mixed resolution in one
     group (128^2 x256, 256^2 x192, 512^2 x64; each step a captured graph per
@@ -819,7 +870,7 @@ def main():
         return
     extra = {"tg2d64": run_tg2d64, "tg3d-accuracy": run_tg3d_accuracy, "dsl-ensemble": run_dsl_ensemble,
              "fbm512": run_fbm512, "serving": run_serving, "dft-gemm-stage": run_dft_gemm_stage,
-             "exchange": run_exchange}
+             "exchange": run_exchange, "dsl-classes": run_dsl_classes}
     if args.workload in extra:
         import torch
         torch.cuda.set_device(local)
