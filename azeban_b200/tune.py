@@ -1,9 +1,10 @@
 """Autotuner for the radix plans of the transform passes.
 
-For one workload (dimension, N, padded M, precision, batch) it runs the
-right-hand side with every plan variant, times each pass with the library's
-per-pass CUDA events (az_profile_*), and keeps, for each pass kind (column
-passes, contiguous-axis product pass, epilogue pass), the faster variant.
+For one workload (dimension, N, padded M, precision, batch) it runs SSP-RK3
+steps of a Simulation with every kernel variant, times each pass with the
+library's per-pass CUDA events (az_profile_*), and keeps, for each pass kind
+(column passes, contiguous-axis product pass, epilogue pass), the fastest
+variant.
 Results go into a JSON tuning table that ``azeban_b200`` loads at import
 (``tuning.json`` beside this file) and applies with az_tune_set.
 
