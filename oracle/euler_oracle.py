@@ -382,8 +382,11 @@ class IncompressibleEuler:
         return float(getattr(self.visc_, "eps", 0.0))
 
     def dt(self, C: float) -> float:
-        """C / (N_phys * u_max_) (incompressible_euler.hpp:122-124)."""
-        return C / (self.grid.N_phys * self.u_max_)
+        """C / (N_phys * u_max_) (incompressible_euler.hpp:122-124), in IEEE
+        double arithmetic as the reference computes it: +inf for a zero field
+        (SSP_RK3::integrate then takes max_dt, ssp_rk3.hpp:55)."""
+        with np.errstate(divide="ignore"):
+            return float(np.float64(C) / (np.float64(self.grid.N_phys) * np.float64(self.u_max_)))
 
     # -- pieces of dudt, exposed so tests can check each stage -------------
     def pad(self, u_hat):
